@@ -1,0 +1,181 @@
+// C ABI of libdbmp.so (declarations and contracts in include/dbmp.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "dbmp_internal.cuh"
+
+namespace dbmp {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  set_error("%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  return DBMP_ERR_CUDA;
+}
+
+// launchers (binning.cu, raster.cu)
+size_t bin_workspace_bytes(int N, int T, long long cap);
+int launch_template_bboxes(const float* tmpl, int P, int Ht, int Wt, float* out, cudaStream_t st);
+int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st);
+int launch_prepare(const Geom& g, const float* means2D, const float* radii, const float* rot, const float* opac,
+                   const float* colors, const int* sel, PrimInfo* out, cudaStream_t st);
+int launch_bin(const Geom& g, int bin_mode, const float* means2D, const float* radii, const float* rot,
+               const float* opac, const float* colors, const int* sel, const float* tbbox, PrimInfo* prim_info,
+               int* tile_offsets, int* tile_indices, long long cap, int* total_out, int* overflow_out,
+               void* ws, size_t ws_bytes, cudaStream_t st);
+int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                   const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st);
+int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                    const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
+                    const float* grad_alpha, double* gacc, cudaStream_t st);
+int launch_finalize(const Geom& g, const float* radii, const float* rot, const float* opac, const float* colors,
+                    const double* gacc, float* gm, float* gr, float* grot, float* go, float* gc, cudaStream_t st);
+int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
+                 const float* target, const float* background, float* out_image, double* gacc, double* loss,
+                 cudaStream_t st);
+
+// Validates a canvas description and derives the launch geometry.
+int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
+  if (!cv) { set_error("%s: canvas is null", who); return DBMP_ERR_INVALID; }
+  if (cv->height <= 0 || cv->width <= 0) { set_error("%s: canvas %dx%d is empty", who, cv->height, cv->width); return DBMP_ERR_INVALID; }
+  if (cv->tile_size != 16 && cv->tile_size != 32) { set_error("%s: tile_size %d is not supported (16 or 32)", who, cv->tile_size); return DBMP_ERR_INVALID; }
+  if (cv->num_prims < 0) { set_error("%s: num_prims %d < 0", who, cv->num_prims); return DBMP_ERR_INVALID; }
+  if (cv->num_templates <= 0 || cv->tmpl_h < 2 || cv->tmpl_w < 2) {
+    set_error("%s: template atlas %dx%dx%d is invalid (need P>=1, Ht,Wt>=2)", who, cv->num_templates, cv->tmpl_h, cv->tmpl_w);
+    return DBMP_ERR_INVALID;
+  }
+  if (cv->atlas_kind < DBMP_ATLAS_F32 || cv->atlas_kind > DBMP_ATLAS_BF16_QUAD) { set_error("%s: atlas_kind %d unknown", who, cv->atlas_kind); return DBMP_ERR_INVALID; }
+  if (!(cv->t_stop >= 1e-30f && cv->t_stop < 1.f)) { set_error("%s: t_stop %g outside [1e-30, 1)", who, (double)cv->t_stop); return DBMP_ERR_INVALID; }
+  if ((long long)cv->height * cv->width > (1ll << 31) / 4) { set_error("%s: canvas too large", who); return DBMP_ERR_INVALID; }
+  g->H = cv->height; g->W = cv->width; g->TS = cv->tile_size;
+  g->tilesX = (cv->width + cv->tile_size - 1) / cv->tile_size;
+  g->tilesY = (cv->height + cv->tile_size - 1) / cv->tile_size;
+  g->T = g->tilesX * g->tilesY;
+  g->N = cv->num_prims; g->P = cv->num_templates; g->Ht = cv->tmpl_h; g->Wt = cv->tmpl_w;
+  g->hx = 0.5f * (float)(cv->tmpl_w - 1);
+  g->hy = 0.5f * (float)(cv->tmpl_h - 1);
+  g->rxy = g->hx / g->hy;
+  g->ryx = g->hy / g->hx;
+  g->alpha_max = cv->alpha_max;
+  g->t_stop = cv->t_stop;
+  return DBMP_OK;
+}
+
+#define REQUIRE(cond, ...) \
+  do { if (!(cond)) { set_error(__VA_ARGS__); return DBMP_ERR_INVALID; } } while (0)
+
+}  // namespace dbmp
+
+using namespace dbmp;
+
+extern "C" {
+
+const char* dbmp_last_error(void) { return g_err; }
+int dbmp_version(void) { return 1; }
+
+int dbmp_num_tiles(const dbmp_canvas* cv) {
+  Geom g;
+  if (make_geom(cv, &g, "dbmp_num_tiles") != DBMP_OK) return -1;
+  return g.T;
+}
+
+size_t dbmp_prim_info_bytes(int num_prims) { return sizeof(PrimInfo) * (size_t)(num_prims > 0 ? num_prims : 0); }
+
+int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* out_bbox, void* stream) {
+  REQUIRE(P >= 0 && Ht >= 2 && Wt >= 2, "dbmp_template_bboxes: bad atlas shape %dx%dx%d", P, Ht, Wt);
+  REQUIRE(P == 0 || (templates && out_bbox), "dbmp_template_bboxes: null pointer");
+  return launch_template_bboxes(templates, P, Ht, Wt, out_bbox, (cudaStream_t)stream);
+}
+
+int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, void* out, void* stream) {
+  REQUIRE(P >= 0 && Ht >= 1 && Wt >= 1, "dbmp_atlas_pack: bad atlas shape %dx%dx%d", P, Ht, Wt);
+  REQUIRE(P == 0 || (templates && out), "dbmp_atlas_pack: null pointer");
+  return launch_atlas_pack(templates, P, Ht, Wt, kind, out, (cudaStream_t)stream);
+}
+
+size_t dbmp_bin_workspace_bytes(const dbmp_canvas* cv, long long capacity) {
+  Geom g;
+  if (make_geom(cv, &g, "dbmp_bin_workspace_bytes") != DBMP_OK) return 0;
+  if (capacity < 0) capacity = 0;
+  return bin_workspace_bytes(g.N, g.T, capacity);
+}
+
+int dbmp_prepare(const dbmp_canvas* cv, const float* means2D, const float* radii, const float* rotations,
+                 const float* opacities, const float* colors, const int32_t* sel, void* prim_info, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_prepare");
+  if (rc) return rc;
+  REQUIRE(g.N == 0 || (means2D && radii && rotations && opacities && colors && sel && prim_info),
+          "dbmp_prepare: null pointer");
+  REQUIRE(((uintptr_t)prim_info & 15) == 0, "dbmp_prepare: prim_info must be 16-byte aligned");
+  return launch_prepare(g, means2D, radii, rotations, opacities, colors, sel, (PrimInfo*)prim_info,
+                        (cudaStream_t)stream);
+}
+
+int dbmp_bin(const dbmp_canvas* cv, const float* means2D, const float* radii, const float* rotations,
+             const float* opacities, const float* colors, const int32_t* sel, const float* tmpl_bbox,
+             void* prim_info, int32_t* tile_offsets, int32_t* tile_indices, long long capacity,
+             int32_t* total_out, int32_t* overflow_out, void* workspace, size_t workspace_bytes, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_bin");
+  if (rc) return rc;
+  REQUIRE(cv->bin_mode == DBMP_BIN_CONTENT || cv->bin_mode == DBMP_BIN_CULL, "dbmp_bin: bin_mode %d unknown", cv->bin_mode);
+  REQUIRE(g.N == 0 || (means2D && radii && rotations && opacities && colors && sel && prim_info),
+          "dbmp_bin: null pointer");
+  REQUIRE(cv->bin_mode != DBMP_BIN_CONTENT || tmpl_bbox, "dbmp_bin: tmpl_bbox is required in DBMP_BIN_CONTENT mode");
+  REQUIRE(tile_offsets && total_out && workspace, "dbmp_bin: null output or workspace");
+  REQUIRE(capacity >= 0 && capacity <= 0x7fffffffll, "dbmp_bin: capacity %lld outside [0, 2^31)", capacity);
+  REQUIRE(capacity == 0 || tile_indices, "dbmp_bin: tile_indices is null");
+  REQUIRE(((uintptr_t)prim_info & 15) == 0 && ((uintptr_t)workspace & 255) == 0,
+          "dbmp_bin: prim_info must be 16-byte and workspace 256-byte aligned");
+  return launch_bin(g, cv->bin_mode, means2D, radii, rotations, opacities, colors, sel, tmpl_bbox,
+                    (PrimInfo*)prim_info, tile_offsets, tile_indices, capacity, total_out, overflow_out, workspace,
+                    workspace_bytes, (cudaStream_t)stream);
+}
+
+int dbmp_forward(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
+                 const int32_t* tile_indices, float* out_color, float* out_alpha, float* T_last, int32_t* last_pos,
+                 void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_forward");
+  if (rc) return rc;
+  REQUIRE(atlas && tile_offsets && tile_indices && out_color && out_alpha && T_last && last_pos,
+          "dbmp_forward: null pointer");
+  REQUIRE(g.N == 0 || prim_info, "dbmp_forward: prim_info is null");
+  return launch_forward(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, out_color,
+                        out_alpha, T_last, last_pos, (cudaStream_t)stream);
+}
+
+int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
+                  const int32_t* tile_indices, const float* T_last, const int32_t* last_pos, const float* grad_color,
+                  const float* grad_alpha, const float* radii, const float* rotations, const float* opacities,
+                  const float* colors, double* grad_accum, float* grad_means2D, float* grad_radii,
+                  float* grad_rotations, float* grad_opacities, float* grad_colors, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_backward");
+  if (rc) return rc;
+  REQUIRE(atlas && tile_offsets && tile_indices && T_last && last_pos && grad_color, "dbmp_backward: null input");
+  REQUIRE(g.N == 0 || (prim_info && radii && rotations && opacities && colors), "dbmp_backward: null parameter");
+  REQUIRE(g.N == 0 || (grad_accum && grad_means2D && grad_radii && grad_rotations && grad_opacities && grad_colors),
+          "dbmp_backward: null output");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (g.N > 0) {
+    cudaError_t e = cudaMemsetAsync(grad_accum, 0, sizeof(double) * 8 * (size_t)g.N, st);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(grad_accum)");
+  }
+  rc = launch_backward(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, T_last,
+                       last_pos, grad_color, grad_alpha, grad_accum, st);
+  if (rc) return rc;
+  return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
+                         grad_rotations, grad_opacities, grad_colors, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,483 @@
+// Forward / backward / fused tile compositing kernels.
+//
+// One CTA of 256 threads owns one tile of TS x TS pixels (TS = 32: four
+// pixels per thread, TS = 16: one).  Each warp owns a compact footprint
+// (16x8 or 8x4 pixels) so that a primitive's square cull is mostly warp
+// uniform and the warp's texel fetches stay close together in the atlas.
+// The tile's primitive list is walked in chunks of CH entries whose 64-byte
+// PrimInfo records are staged in shared memory once per CTA; warps that have
+// finished (every pixel below t_stop) skip the math but keep joining the
+// chunk barriers.
+#include "dbmp_internal.cuh"
+
+namespace dbmp {
+
+constexpr int kThreads = 256;
+constexpr int kChunk = 32;   // list entries staged per barrier
+
+template <int TS> struct PixLayout;
+template <> struct PixLayout<32> { static constexpr int NP = 4, FW = 16, FH = 8; };
+template <> struct PixLayout<16> { static constexpr int NP = 1, FW = 8, FH = 4; };
+
+// Pixel p of this thread inside its tile.
+template <int TS>
+__device__ __forceinline__ void pixel_of(int warp, int lane, int p, int* x, int* y) {
+  using L = PixLayout<TS>;
+  *x = (warp & 1) * L::FW + (lane & 7) + 8 * (p & 1);
+  *y = (warp >> 1) * L::FH + (lane >> 3) + 4 * (p >> 1);
+}
+
+// Stages entries [base, base+n) of the tile list: ids and PrimInfo records.
+__device__ __forceinline__ void stage_chunk(const PrimInfo* __restrict__ prims, const int* __restrict__ idx,
+                                            int N, int base, int n, float4 (*s_pi)[4], int* s_id) {
+  const int e = threadIdx.x >> 2, q = threadIdx.x & 3;
+  if (e < n) {
+    const int id = __ldg(idx + base + e);
+    float4 v;
+    if (id >= 0 && id < N) {
+      v = __ldg(reinterpret_cast<const float4*>(prims + id) + q);
+    } else {  // out-of-range ids are skipped like tile_forward.cu:184-185
+      v = make_float4(0.f, 0.f, -1.f, -1.f);
+      if (q == 3) v.x = __int_as_float(-1);
+    }
+    s_pi[e][q] = v;
+    if (q == 0) s_id[e] = (id >= 0 && id < N) ? id : -1;
+  }
+}
+
+// Conservative warp-uniform rejection: true when the primitive's cull square
+// misses every pixel of the warp footprint (1 px margin for rounding; NaN
+// never rejects, matching the reference's cull).
+__device__ __forceinline__ bool footprint_miss(const float4& g0, float x0, float x1, float y0, float y1) {
+  return (g0.x - g0.z > x1 + 1.f) || (g0.x + g0.z < x0 - 1.f) || (g0.y - g0.w > y1 + 1.f) ||
+         (g0.y + g0.w < y0 - 1.f);
+}
+
+// ---------------------------------------------------------------------------
+// Forward walk for one tile.  Leaves per-pixel colour, final T, the T entering
+// the last contributor and the last contributor's list position.
+template <int TS, int KIND>
+struct TileWalker {
+  using L = PixLayout<TS>;
+  static constexpr int NP = L::NP;
+
+  int warp, lane, start, end;
+  int px[NP], py[NP];
+  bool valid[NP];
+  float fx0, fx1, fy0, fy1;
+
+  __device__ __forceinline__ void init(const Geom& g, int tile, const int* __restrict__ offs) {
+    warp = threadIdx.x >> 5;
+    lane = threadIdx.x & 31;
+    const int tx = tile % g.tilesX, ty = tile / g.tilesX;
+    start = __ldg(offs + tile);
+    end = __ldg(offs + tile + 1);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      int x, y;
+      pixel_of<TS>(warp, lane, p, &x, &y);
+      px[p] = tx * TS + x;
+      py[p] = ty * TS + y;
+      valid[p] = px[p] < g.W && py[p] < g.H;
+    }
+    fx0 = (float)(tx * TS + (warp & 1) * L::FW);
+    fx1 = fx0 + (float)(L::FW - 1);
+    fy0 = (float)(ty * TS + (warp >> 1) * L::FH);
+    fy1 = fy0 + (float)(L::FH - 1);
+  }
+
+  __device__ __forceinline__ void forward(const Geom& g, const PrimInfo* __restrict__ prims,
+                                          const void* __restrict__ atlas, const int* __restrict__ idx,
+                                          float4 (*s_pi)[4], int* s_id,
+                                          float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP]) {
+    bool done[NP];
+    bool all_done = true;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      C[p][0] = C[p][1] = C[p][2] = 0.f;
+      T[p] = 1.f; Tl[p] = 1.f; lp[p] = -1;
+      done[p] = !valid[p];
+      all_done = all_done && done[p];
+    }
+    bool warp_done = __all_sync(0xffffffffu, all_done);
+    for (int base = start; base < end; base += kChunk) {
+      const int n = min(kChunk, end - base);
+      stage_chunk(prims, idx, g.N, base, n, s_pi, s_id);
+      __syncthreads();
+      if (!warp_done) {
+        for (int e = 0; e < n; ++e) {
+          const float4 g0 = s_pi[e][0];
+          if (footprint_miss(g0, fx0, fx1, fy0, fy1)) continue;
+          const int tmpl = __float_as_int(s_pi[e][3].x);
+          if (tmpl < 0) continue;
+          const float4 g1 = s_pi[e][1];
+          const float4 g2 = s_pi[e][2];
+          const int pos = base - start + e;
+          bool local_done = true;
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            if (!done[p]) {
+              const float dx = (float)px[p] - g0.x, dy = (float)py[p] - g0.y;
+              if (!(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
+                const float tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
+                const float ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
+                const float m = sample_mask<KIND, false>(atlas, tmpl, g.Ht, g.Wt, tx, ty, nullptr, nullptr);
+                if (m > 1e-6f) {
+                  const float a = g2.x * m;
+                  const float w = T[p] * a;
+                  C[p][0] = fmaf(w, g2.y, C[p][0]);
+                  C[p][1] = fmaf(w, g2.z, C[p][1]);
+                  C[p][2] = fmaf(w, g2.w, C[p][2]);
+                  Tl[p] = T[p];
+                  lp[p] = pos;
+                  T[p] *= fmaxf(1.f - a, 0.f);
+                  if (T[p] < g.t_stop) done[p] = true;
+                }
+              }
+            }
+            local_done = local_done && done[p];
+          }
+          if (__all_sync(0xffffffffu, local_done)) { warp_done = true; break; }
+        }
+      }
+      if (__syncthreads_and(warp_done)) break;
+    }
+  }
+
+  // Reverse walk.  gC/gA are the upstream gradients of each pixel.  Partial
+  // per-primitive sums are reduced in the warp, then across the CTA, and
+  // accumulated into gacc (N,8) f64.
+  __device__ __forceinline__ void backward(const Geom& g, const PrimInfo* __restrict__ prims,
+                                           const void* __restrict__ atlas, const int* __restrict__ idx,
+                                           float4 (*s_pi)[4], int* s_id, float (*s_part)[kChunk][8],
+                                           int* s_kmax, const float (&gC)[NP][3], const float (&gA)[NP],
+                                           const float (&Tl)[NP], const int (&lp)[NP], double* __restrict__ gacc) {
+    int my_max = -1;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) my_max = max(my_max, lp[p]);
+    const int warp_max = __reduce_max_sync(0xffffffffu, my_max);
+    if (threadIdx.x == 0) *s_kmax = -1;
+    __syncthreads();
+    if (lane == 0) atomicMax(s_kmax, warp_max);
+    __syncthreads();
+    const int kmax = *s_kmax;
+    if (kmax < 0) return;
+
+    float Ts[NP], R[NP][3], B[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      Ts[p] = Tl[p];
+      R[p][0] = R[p][1] = R[p][2] = 0.f;
+      B[p] = 1.f;
+    }
+    for (int cb = (kmax / kChunk) * kChunk; cb >= 0; cb -= kChunk) {
+      const int n = min(kChunk, end - start - cb);
+      stage_chunk(prims, idx, g.N, start + cb, n, s_pi, s_id);
+      __syncthreads();
+      for (int e = n - 1; e >= 0; --e) {
+        const int pos = cb + e;
+        float acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = 0.f;
+        bool any = false;
+        const float4 g0 = s_pi[e][0];
+        const int tmpl = __float_as_int(s_pi[e][3].x);
+        if (pos <= warp_max && tmpl >= 0 && !footprint_miss(g0, fx0, fx1, fy0, fy1)) {
+          const float4 g1 = s_pi[e][1];
+          const float4 g2 = s_pi[e][2];
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            if (pos <= lp[p]) {
+              const float dx = (float)px[p] - g0.x, dy = (float)py[p] - g0.y;
+              if (!(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
+                const float tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
+                const float ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
+                float gx, gy;
+                const float m = sample_mask<KIND, true>(atlas, tmpl, g.Ht, g.Wt, tx, ty, &gx, &gy);
+                if (m > 1e-6f) {
+                  const float a = g2.x * m;
+                  const float om = fmaxf(1.f - a, 0.f);
+                  // T entering this fragment: stored for the last contributor,
+                  // otherwise undo the forward product (om >= t_stop > 0 here).
+                  const float Tk = (pos == lp[p]) ? Tl[p] : __fdiv_rn(Ts[p], om);
+                  Ts[p] = Tk;
+                  const float G = gC[p][0] * (g2.y - R[p][0]) + gC[p][1] * (g2.z - R[p][1]) +
+                                  gC[p][2] * (g2.w - R[p][2]) + gA[p] * B[p];
+                  const float dLda = Tk * G;
+                  const float ex = tx - g.hx, ey = ty - g.hy;
+                  acc[0] = fmaf(dLda, gx, acc[0]);
+                  acc[1] = fmaf(dLda, gy, acc[1]);
+                  acc[2] = fmaf(dLda, fmaf(gx, ex, gy * ey), acc[2]);
+                  acc[3] = fmaf(dLda, fmaf(gx * ey, g.rxy, -gy * ex * g.ryx), acc[3]);
+                  const float w = a * Tk;
+                  acc[4] = fmaf(gC[p][0], w, acc[4]);
+                  acc[5] = fmaf(gC[p][1], w, acc[5]);
+                  acc[6] = fmaf(gC[p][2], w, acc[6]);
+                  acc[7] = fmaf(dLda, a, acc[7]);
+                  R[p][0] = fmaf(om, R[p][0], g2.y * a);
+                  R[p][1] = fmaf(om, R[p][1], g2.z * a);
+                  R[p][2] = fmaf(om, R[p][2], g2.w * a);
+                  B[p] *= om;
+                  any = true;
+                }
+              }
+            }
+          }
+        }
+        if (__any_sync(0xffffffffu, any)) {
+          // recursive-halving reduction: 8 sums over 32 lanes in 9 shuffles;
+          // lane l (l < 8) ends with sum index 4*(l&1) + 2*((l>>1)&1) + ((l>>2)&1)
+          const bool b0 = lane & 1, b1 = lane & 2, b2 = lane & 4;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const float send = b0 ? acc[k] : acc[k + 4];
+            const float keep = b0 ? acc[k + 4] : acc[k];
+            acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+          }
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const float send = b1 ? acc[k] : acc[k + 2];
+            const float keep = b1 ? acc[k + 2] : acc[k];
+            acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+          }
+          {
+            const float send = b2 ? acc[0] : acc[1];
+            const float keep = b2 ? acc[1] : acc[0];
+            acc[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+          }
+          acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 8);
+          acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 16);
+          if (lane < 8) s_part[warp][e][4 * (lane & 1) + 2 * ((lane >> 1) & 1) + ((lane >> 2) & 1)] = acc[0];
+        } else if (lane < 8) {
+          s_part[warp][e][lane] = 0.f;
+        }
+      }
+      __syncthreads();
+      // CTA reduction over the 8 warps; one f64 atomic per non-zero sum.
+      for (int i = threadIdx.x; i < n * 8; i += kThreads) {
+        const int e = i >> 3, k = i & 7;
+        float s = 0.f;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) s += s_part[w][e][k];
+        if (s != 0.f && s_id[e] >= 0) atomicAdd(gacc + (size_t)s_id[e] * 8 + k, (double)s);
+      }
+      __syncthreads();
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+template <int TS, int KIND>
+__global__ void __launch_bounds__(kThreads) forward_kernel(Geom g, const PrimInfo* __restrict__ prims,
+                                                           const void* __restrict__ atlas,
+                                                           const int* __restrict__ offs, const int* __restrict__ idx,
+                                                           float* __restrict__ out_color, float* __restrict__ out_alpha,
+                                                           float* __restrict__ T_last, int* __restrict__ last_pos) {
+  __shared__ float4 s_pi[kChunk][4];
+  __shared__ int s_id[kChunk];
+  TileWalker<TS, KIND> tw;
+  tw.init(g, blockIdx.x, offs);
+  constexpr int NP = TileWalker<TS, KIND>::NP;
+  float C[NP][3], T[NP], Tl[NP];
+  int lp[NP];
+  tw.forward(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp);
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    if (!tw.valid[p]) continue;
+    const size_t q = (size_t)tw.py[p] * g.W + tw.px[p];
+    out_color[3 * q + 0] = C[p][0];
+    out_color[3 * q + 1] = C[p][1];
+    out_color[3 * q + 2] = C[p][2];
+    out_alpha[q] = 1.f - T[p];
+    T_last[q] = Tl[p];
+    last_pos[q] = lp[p];
+  }
+}
+
+template <int TS, int KIND>
+__global__ void __launch_bounds__(kThreads) backward_kernel(Geom g, const PrimInfo* __restrict__ prims,
+                                                            const void* __restrict__ atlas,
+                                                            const int* __restrict__ offs, const int* __restrict__ idx,
+                                                            const float* __restrict__ T_last,
+                                                            const int* __restrict__ last_pos,
+                                                            const float* __restrict__ grad_color,
+                                                            const float* __restrict__ grad_alpha,
+                                                            double* __restrict__ gacc) {
+  __shared__ float4 s_pi[kChunk][4];
+  __shared__ int s_id[kChunk];
+  __shared__ float s_part[kThreads / 32][kChunk][8];
+  __shared__ int s_kmax;
+  TileWalker<TS, KIND> tw;
+  tw.init(g, blockIdx.x, offs);
+  constexpr int NP = TileWalker<TS, KIND>::NP;
+  float gC[NP][3], gA[NP], Tl[NP];
+  int lp[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    if (tw.valid[p]) {
+      const size_t q = (size_t)tw.py[p] * g.W + tw.px[p];
+      gC[p][0] = grad_color[3 * q + 0];
+      gC[p][1] = grad_color[3 * q + 1];
+      gC[p][2] = grad_color[3 * q + 2];
+      gA[p] = grad_alpha ? grad_alpha[q] : 0.f;
+      Tl[p] = T_last[q];
+      lp[p] = last_pos[q];
+    } else {
+      gC[p][0] = gC[p][1] = gC[p][2] = 0.f;
+      gA[p] = 0.f; Tl[p] = 1.f; lp[p] = -1;
+    }
+  }
+  tw.backward(g, prims, atlas, idx, s_pi, s_id, s_part, &s_kmax, gC, gA, Tl, lp, gacc);
+}
+
+__device__ __forceinline__ double sigmoid_d(double x) {
+  if (x >= 0.0) { const double z = exp(-x); return 1.0 / (1.0 + z); }
+  const double z = exp(x);
+  return z / (1.0 + z);
+}
+
+// Converts the accumulated per-primitive sums into the reference's gradient
+// outputs (tile_backward.cu:255-343 chain rule, applied once per primitive).
+__global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const float* __restrict__ rot,
+                                const float* __restrict__ opac, const float* __restrict__ colors,
+                                const double* __restrict__ gacc, float* __restrict__ g_means,
+                                float* __restrict__ g_radii, float* __restrict__ g_rot, float* __restrict__ g_opac,
+                                float* __restrict__ g_colors) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= g.N) return;
+  const double* S = gacc + (size_t)n * 8;
+  const float r = radii[n];
+  const double rinv = (r > 1e-6f) ? 1.0 / (double)r : 1e6;
+  double s, c;
+  sincos((double)rot[n], &s, &c);
+  const double sv = sigmoid_d((double)opac[n]);
+  const double a0 = (double)g.alpha_max * sv;
+  const double hx = g.hx, hy = g.hy;
+  g_means[2 * n + 0] = (float)(a0 * rinv * (-c * hx * S[0] + s * hy * S[1]));
+  g_means[2 * n + 1] = (float)(a0 * rinv * (-s * hx * S[0] - c * hy * S[1]));
+  g_radii[n] = (float)(-a0 * rinv * S[2]);
+  g_rot[n] = (float)(a0 * S[3]);
+  g_opac[n] = (float)((1.0 - sv) * S[7]);
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    const double sc = sigmoid_d((double)colors[3 * n + ch]);
+    g_colors[3 * n + ch] = (float)(sc * (1.0 - sc) * S[4 + ch]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused forward + L2 loss + backward for image fitting.  The loss is the
+// reference's mse_loss(rendered, target) (pydiffbmp/util/loss_functions.py:20-40)
+// on rendered = C + (1 - A) * background (simple_tile_renderer.py:704-707):
+//   dL/dC = 2 (rendered - target) / (3HW),  dL/dA = -sum_c dL/dC_c * bg_c.
+// loss_out (f64, may be null) receives sum((rendered - target)^2) / (3HW).
+template <int TS, int KIND>
+__global__ void __launch_bounds__(kThreads) fused_kernel(Geom g, const PrimInfo* __restrict__ prims,
+                                                         const void* __restrict__ atlas,
+                                                         const int* __restrict__ offs, const int* __restrict__ idx,
+                                                         const float* __restrict__ target,
+                                                         const float* __restrict__ background,
+                                                         float* __restrict__ out_image, double* __restrict__ gacc,
+                                                         double* __restrict__ loss_out) {
+  __shared__ float4 s_pi[kChunk][4];
+  __shared__ int s_id[kChunk];
+  __shared__ float s_part[kThreads / 32][kChunk][8];
+  __shared__ int s_kmax;
+  __shared__ float s_loss[kThreads / 32];
+  TileWalker<TS, KIND> tw;
+  tw.init(g, blockIdx.x, offs);
+  constexpr int NP = TileWalker<TS, KIND>::NP;
+  float C[NP][3], T[NP], Tl[NP], gC[NP][3], gA[NP];
+  int lp[NP];
+  tw.forward(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp);
+  const float inv = 1.f / (3.f * (float)g.H * (float)g.W);
+  float lsum = 0.f;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    gA[p] = 0.f;
+    gC[p][0] = gC[p][1] = gC[p][2] = 0.f;
+    if (!tw.valid[p]) continue;
+    const size_t q = (size_t)tw.py[p] * g.W + tw.px[p];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      const float bg = background ? background[3 * q + ch] : 0.f;
+      const float img = fmaf(T[p], bg, C[p][ch]);
+      if (out_image) out_image[3 * q + ch] = img;
+      const float d = img - target[3 * q + ch];
+      lsum = fmaf(d, d, lsum);
+      gC[p][ch] = 2.f * d * inv;
+      gA[p] -= gC[p][ch] * bg;
+    }
+  }
+  if (loss_out) {
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 16);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 8);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 4);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 2);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 1);
+    if (tw.lane == 0) s_loss[tw.warp] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) t += s_loss[w];
+      atomicAdd(loss_out, t * (double)inv);
+    }
+  }
+  tw.backward(g, prims, atlas, idx, s_pi, s_id, s_part, &s_kmax, gC, gA, Tl, lp, gacc);
+}
+
+// ---------------------------------------------------------------------------
+#define DBMP_KIND_SWITCH(kind, ...)                                  \
+  switch (kind) {                                                    \
+    case ATLAS_F32: { constexpr int KD = ATLAS_F32; __VA_ARGS__; } break;             \
+    case ATLAS_F32_QUAD: { constexpr int KD = ATLAS_F32_QUAD; __VA_ARGS__; } break;   \
+    case ATLAS_F16_QUAD: { constexpr int KD = ATLAS_F16_QUAD; __VA_ARGS__; } break;   \
+    case ATLAS_BF16_QUAD: { constexpr int KD = ATLAS_BF16_QUAD; __VA_ARGS__; } break; \
+    default: set_error("unknown atlas kind %d", kind); return DBMP_ERR_INVALID;       \
+  }
+
+#define DBMP_TS_SWITCH(ts, ...)                                      \
+  if ((ts) == 32) { constexpr int TSV = 32; __VA_ARGS__; }           \
+  else if ((ts) == 16) { constexpr int TSV = 16; __VA_ARGS__; }      \
+  else { set_error("tile_size %d is not supported (16 or 32)", ts); return DBMP_ERR_INVALID; }
+
+int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                   const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st) {
+  if (g.T == 0) return DBMP_OK;
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+                                                   g, prims, atlas, offs, idx, color, alpha, T_last, last_pos))));
+  DBMP_CHECK_LAUNCH("forward_kernel");
+  return DBMP_OK;
+}
+
+int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                    const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
+                    const float* grad_alpha, double* gacc, cudaStream_t st) {
+  if (g.T == 0) return DBMP_OK;
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+                                                   g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
+                                                   grad_alpha, gacc))));
+  DBMP_CHECK_LAUNCH("backward_kernel");
+  return DBMP_OK;
+}
+
+int launch_finalize(const Geom& g, const float* radii, const float* rot, const float* opac, const float* colors,
+                    const double* gacc, float* gm, float* gr, float* grot, float* go, float* gc, cudaStream_t st) {
+  if (g.N == 0) return DBMP_OK;
+  finalize_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(g, radii, rot, opac, colors, gacc, gm, gr, grot, go, gc);
+  DBMP_CHECK_LAUNCH("finalize_kernel");
+  return DBMP_OK;
+}
+
+int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
+                 const float* target, const float* background, float* out_image, double* gacc, double* loss,
+                 cudaStream_t st) {
+  if (g.T == 0) return DBMP_OK;
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (fused_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+                                                   g, prims, atlas, offs, idx, target, background, out_image,
+                                                   gacc, loss))));
+  DBMP_CHECK_LAUNCH("fused_kernel");
+  return DBMP_OK;
+}
+
+}  // namespace dbmp

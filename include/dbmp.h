@@ -1,0 +1,150 @@
+/*
+ * dbmp.h -- C ABI of the DiffBMP B200 tile rasterizer (libdbmp.so).
+ *
+ * Plain pointers and sizes only: every array argument is a device pointer
+ * (CUDA global memory of the current device) unless the comment says "host".
+ * `stream` is a cudaStream_t passed as void*.  No entry point synchronises the
+ * device or reads device memory from the host; all work is stream-ordered.
+ * Every call returns a dbmp_status; on failure dbmp_last_error() describes it
+ * (thread-local string).  There is no fallback path: a failed call leaves its
+ * outputs undefined.
+ *
+ * Primitive parameters use the reference's layout and meaning
+ * (smhongok/diffbmp, cuda_tile_rasterizer/ext.cpp:11-28):
+ *   means2D (N,2) f32 pixel centres; radii (N) f32 half extent of the
+ *   template square; rotations (N) f32 radians; opacities (N) f32 logits;
+ *   colors (N,3) f32 logits; sel (N) i32 template id per primitive.
+ * Tile lists use the reference's CSR form: offsets (T+1) i32 and indices (L)
+ * i32, tiles row-major with tile_size x tile_size pixels, primitive ids
+ * ascending within a tile (pydiffbmp/core/renderer/simple_tile_renderer.py:721-766).
+ */
+#ifndef DBMP_H
+#define DBMP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DBMP_OK = 0,
+  DBMP_ERR_INVALID = 1,      /* bad argument (size, null pointer, unsupported tile size) */
+  DBMP_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed */
+  DBMP_ERR_CAPACITY = 3,     /* caller buffer too small (see the entry point) */
+  DBMP_ERR_UNSUPPORTED = 4   /* feature combination not built */
+} dbmp_status;
+
+/* Atlas storage kinds (dbmp_canvas.atlas_kind). */
+#define DBMP_ATLAS_F32 0        /* (P,Ht,Wt) f32, the reference layout */
+#define DBMP_ATLAS_F32_QUAD 1   /* (P,Ht,Wt,4) f32 bilinear quads, see dbmp_atlas_pack */
+#define DBMP_ATLAS_F16_QUAD 2   /* (P,Ht,Wt,4) IEEE half quads */
+#define DBMP_ATLAS_BF16_QUAD 3  /* (P,Ht,Wt,4) bfloat16 quads */
+
+/* Binning modes (dbmp_canvas.bin_mode). */
+#define DBMP_BIN_CONTENT 0  /* world bbox of the template's texels > 1e-6:
+                               pydiffbmp/core/renderer/vector_renderer.py:194-252,401-444 */
+#define DBMP_BIN_CULL 1     /* square cull box: the tight equivalent of the
+                               all-primitives default mapping of
+                               cuda_tile_rasterizer/tile_rasterize.cu:171-194 */
+
+typedef struct {
+  int32_t height, width;      /* canvas in pixels */
+  int32_t tile_size;          /* 16 or 32 */
+  int32_t num_prims;          /* N */
+  int32_t num_templates;      /* P */
+  int32_t tmpl_h, tmpl_w;     /* Ht, Wt */
+  int32_t atlas_kind;         /* DBMP_ATLAS_* */
+  int32_t bin_mode;           /* DBMP_BIN_* */
+  float alpha_max;            /* alpha_upper_bound */
+  float t_stop;               /* early-termination transmittance, in [1e-30, 1) */
+  int32_t reserved;
+} dbmp_canvas;
+
+const char* dbmp_last_error(void);
+int dbmp_version(void);
+/* Number of tiles of a canvas: ceil(H/ts)*ceil(W/ts). */
+int dbmp_num_tiles(const dbmp_canvas* cv);
+
+/* Per-template bbox of texels > 1e-6 in normalised [-1,1] coordinates,
+ * (P,4) f32 [min_u, max_u, min_v, max_v]; (-1,1,-1,1) for an empty template.
+ * Replaces SimpleTileRenderer._compute_primitive_bboxes
+ * (pydiffbmp/core/renderer/simple_tile_renderer.py:130-171), bit-exact. */
+int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* out_bbox,
+                         void* stream);
+
+/* Repacks a (P,Ht,Wt) f32 atlas into kind DBMP_ATLAS_{F32,F16,BF16}_QUAD:
+ * element (p,y,x) holds the bilinear neighbours t[y][x], t[y][x+1],
+ * t[y+1][x], t[y+1][x+1] (0 outside the template).  out holds P*Ht*Wt*4
+ * elements of the kind's type.  No reference counterpart (storage format of
+ * the precision form). */
+int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, void* out, void* stream);
+
+/* Scratch bytes that dbmp_bin needs for `capacity` tile-list entries. */
+size_t dbmp_bin_workspace_bytes(const dbmp_canvas* cv, long long capacity);
+/* Bytes of the per-primitive record array written by dbmp_bin / dbmp_prepare. */
+size_t dbmp_prim_info_bytes(int num_prims);
+
+/* Per-primitive preparation only (for callers that supply their own tile
+ * lists): fills prim_info (dbmp_prim_info_bytes(N) bytes, 16-byte aligned). */
+int dbmp_prepare(const dbmp_canvas* cv, const float* means2D, const float* radii,
+                 const float* rotations, const float* opacities, const float* colors,
+                 const int32_t* sel, void* prim_info, void* stream);
+
+/* Device binning: preparation + per-primitive tile rectangles + stable key
+ * sort by tile -> CSR tile lists.  Writes prim_info, tile_offsets (T+1),
+ * tile_indices (first L of `capacity` entries) and *total_out (device int32,
+ * = L).  When L > capacity the lists are not written, *total_out still holds
+ * L and *overflow_out (device int32, may be null) is set to 1; call again with
+ * capacity >= L.  capacity == 0 only counts.  tmpl_bbox is the output of
+ * dbmp_template_bboxes (only read in DBMP_BIN_CONTENT mode).
+ * Replaces VectorRenderer._unified_primitive_assignment
+ * (pydiffbmp/core/renderer/vector_renderer.py:401-444) followed by
+ * SimpleTileRenderer._convert_masks_to_mapping (simple_tile_renderer.py:721-766);
+ * tile lists are bit-identical to the reference's in DBMP_BIN_CONTENT mode. */
+int dbmp_bin(const dbmp_canvas* cv, const float* means2D, const float* radii,
+             const float* rotations, const float* opacities, const float* colors,
+             const int32_t* sel, const float* tmpl_bbox, void* prim_info,
+             int32_t* tile_offsets, int32_t* tile_indices, long long capacity,
+             int32_t* total_out, int32_t* overflow_out, void* workspace, size_t workspace_bytes,
+             void* stream);
+
+/* Forward compositing.  out_color (H,W,3) f32 = sum_k T_k a_k c_k and
+ * out_alpha (H,W) f32 = 1 - T_final, front to back over each tile's list,
+ * stopping a pixel once T < t_stop.  Per pixel it also stores the
+ * transmittance entering the last contributor (T_last, f32) and that
+ * contributor's position in the tile list (last_pos, i32, -1 if none); the
+ * backward recomputes everything else from these.
+ * Replaces CudaRasterizeTilesForwardKernel
+ * (cuda_tile_rasterizer/cuda_kernels/tile_forward.h:6-11) as called by
+ * TileRasterizer::forward (cuda_tile_rasterizer/tile_rasterize.cu:297-498). */
+int dbmp_forward(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+                 const int32_t* tile_offsets, const int32_t* tile_indices,
+                 float* out_color, float* out_alpha, float* T_last, int32_t* last_pos,
+                 void* stream);
+
+/* Backward.  Reverse traversal from each pixel's last contributor,
+ * recovering T_k from T_last; per-primitive sums are warp/CTA reduced and
+ * accumulated in grad_accum ((N,8) f64 scratch, zeroed by this call), then
+ * converted, with the primitives' radii / rotations / opacity and colour
+ * logits, into the reference's five gradient outputs (f32, overwritten):
+ * grad_means2D (N,2), grad_radii (N), grad_rotations (N),
+ * grad_opacities (N), grad_colors (N,3).  grad_alpha may be null.
+ * Replaces CudaRasterizeTilesBackwardKernel
+ * (cuda_tile_rasterizer/cuda_kernels/tile_backward.h:6-14) as called by
+ * TileRasterizer::backward (cuda_tile_rasterizer/tile_rasterize.cu:638-780). */
+int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+                  const int32_t* tile_offsets, const int32_t* tile_indices,
+                  const float* T_last, const int32_t* last_pos,
+                  const float* grad_color, const float* grad_alpha,
+                  const float* radii, const float* rotations, const float* opacities,
+                  const float* colors, double* grad_accum,
+                  float* grad_means2D, float* grad_radii, float* grad_rotations,
+                  float* grad_opacities, float* grad_colors, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DBMP_H */

@@ -1,0 +1,194 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference's own
+Python code (smhongok/diffbmp, pydiffbmp package) on the CPU.
+
+Run by hand in a checkout that has the reference next to it:
+
+    python tests/golden/make_golden.py --reference /path/to/diffbmp
+
+The reference's optional dependencies that are absent here (cairosvg,
+psd_tools, piq, ...) are replaced by empty stub modules; none of them is on
+the code paths exercised below.  Fixtures produced:
+
+* tmpl_bbox.npz   -- SimpleTileRenderer._compute_primitive_bboxes
+                     (pydiffbmp/core/renderer/simple_tile_renderer.py:130-171)
+* bin_<case>.npz  -- _unified_primitive_assignment + _convert_masks_to_mapping
+                     (vector_renderer.py:401-444, simple_tile_renderer.py:721-766)
+* torch_<case>.npz -- the PyTorch per-tile renderer (_process_tiles_parallel with
+                     CUDA off, simple_tile_renderer.py:479-569, 1304-1550):
+                     image, alpha and autograd gradients of
+                     sum(image*wc) + sum(alpha*wa) for seeded weights wc, wa.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.abc
+import importlib.machinery
+import os
+import sys
+from unittest import mock
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+_STUBS = {"cairosvg", "psd_tools", "piq", "matplotlib", "svgpathtools", "svgwrite", "scour",
+          "fontTools", "pyvista", "moviepy", "pylrc", "wandb", "clip", "lpips"}
+
+
+class _StubFinder(importlib.abc.MetaPathFinder, importlib.abc.Loader):
+    def find_spec(self, name, path, target=None):
+        if name.split(".")[0] in _STUBS:
+            return importlib.machinery.ModuleSpec(name, self, is_package=True)
+        return None
+
+    def create_module(self, spec):
+        m = mock.MagicMock()
+        m.__path__ = []
+        m.__spec__ = spec
+        m.__name__ = spec.name
+        return m
+
+    def exec_module(self, module):
+        pass
+
+
+def load_reference(ref_root: str):
+    os.environ["WANDB_MODE"] = "disabled"
+    sys.meta_path.insert(0, _StubFinder())
+    sys.path.insert(0, ref_root)
+    import torch  # noqa: F401
+    from pydiffbmp.core.renderer import simple_tile_renderer as str_
+    str_.CUDA_AVAILABLE = False      # take the PyTorch per-tile path
+    return str_
+
+
+def make_renderer(str_, H, W, S, ts, amax):
+    import torch
+    P, Ht, Wt = S.shape
+    co = torch.zeros(P, Ht, Wt, 3)
+    R = str_.SimpleTileRenderer((H, W), torch.from_numpy(S), tile_size=ts, alpha_upper_bound=amax,
+                                device="cpu", c_blend=-40.0, primitive_colors=co)
+    R._forward_compute_time_accum = 0.0
+    return R
+
+
+def tile_bounds(H, W, ts):
+    import torch
+    th, tw = (H + ts - 1) // ts, (W + ts - 1) // ts
+    ty = torch.arange(th).repeat_interleave(tw)
+    tx = torch.arange(tw).repeat(th)
+    ys = ty * ts
+    ye = torch.clamp(ys + ts, max=H)
+    xs = tx * ts
+    xe = torch.clamp(xs + ts, max=W)
+    return xs, xe, ys, ye
+
+
+def scene_params(rng, H, W, N, rmin, rmax, off_canvas=0.0):
+    cx = rng.uniform(-off_canvas * W, (1 + off_canvas) * W, N)
+    cy = rng.uniform(-off_canvas * H, (1 + off_canvas) * H, N)
+    r = np.exp(rng.uniform(np.log(rmin), np.log(rmax), N))
+    th = rng.uniform(0, 2 * np.pi, N)
+    v = rng.normal(0, 1.2, N)
+    c = rng.normal(0, 1.5, (N, 3))
+    return (np.stack([cx, cy], 1).astype(np.float32), r.astype(np.float32), th.astype(np.float32),
+            v.astype(np.float32), c.astype(np.float32))
+
+
+def gen_bin_case(str_, name, H, W, ts, S, N, seed, rmin, rmax, off_canvas=0.0, special=None):
+    import torch
+    rng = np.random.default_rng(seed)
+    means2D, r, th, v, c = scene_params(rng, H, W, N, rmin, rmax, off_canvas)
+    if special is not None:
+        special(means2D, r, th)
+    R = make_renderer(str_, H, W, S, ts, 1.0)
+    xs, xe, ys, ye = tile_bounds(H, W, ts)
+    x = torch.from_numpy(means2D[:, 0].copy()); y = torch.from_numpy(means2D[:, 1].copy())
+    masks = R._unified_primitive_assignment(x, y, torch.from_numpy(r), torch.from_numpy(th),
+                                            xs, xe, ys, ye)
+    mapping = R._convert_masks_to_mapping(masks, xs, xe, ys, ye).numpy().astype(np.int32)
+    np.savez_compressed(os.path.join(HERE, f"bin_{name}.npz"), H=H, W=W, ts=ts, S=S,
+                        means2D=means2D, radii=r, rotations=th, mapping=mapping,
+                        tbbox=np.array(R.primitive_bboxes, np.float32))
+    print(f"bin_{name}: N={N} L={mapping[1]}")
+
+
+def gen_torch_case(str_, name, H, W, ts, S, N, seed, rmin, rmax, amax):
+    import torch
+    rng = np.random.default_rng(seed)
+    means2D, r, th, v, c = scene_params(rng, H, W, N, rmin, rmax)
+    P = S.shape[0]
+    R = make_renderer(str_, H, W, S, ts, amax)
+    x = torch.tensor(means2D[:, 0], requires_grad=True)
+    y = torch.tensor(means2D[:, 1], requires_grad=True)
+    rr = torch.tensor(r, requires_grad=True)
+    tt = torch.tensor(th, requires_grad=True)
+    vv = torch.tensor(v, requires_grad=True)
+    cc = torch.tensor(c, requires_grad=True)
+    gsel = (torch.arange(N) % P).flip(0)
+    out = torch.zeros(H, W, 3)
+    img, alpha = R._process_tiles_parallel(x, y, rr, tt, vv, cc, 0.0, None, gsel, out, None,
+                                           return_alpha=True)
+    wc = torch.from_numpy(rng.normal(0, 1, (H, W, 3)).astype(np.float32))
+    wa = torch.from_numpy(rng.normal(0, 1, (H, W)).astype(np.float32))
+    ((img * wc).sum() + (alpha * wa).sum()).backward()
+    xs, xe, ys, ye = tile_bounds(H, W, ts)
+    masks = R._unified_primitive_assignment(x.detach(), y.detach(), rr.detach(), tt.detach(),
+                                            xs, xe, ys, ye)
+    mapping = R._convert_masks_to_mapping(masks, xs, xe, ys, ye).numpy().astype(np.int32)
+    np.savez_compressed(
+        os.path.join(HERE, f"torch_{name}.npz"), H=H, W=W, ts=ts, S=S, amax=amax,
+        means2D=means2D, radii=r, rotations=th, opacities=v, colors=c, sel=gsel.numpy().astype(np.int32),
+        mapping=mapping, image=img.detach().numpy(), alpha=alpha.detach().numpy(),
+        wc=wc.numpy(), wa=wa.numpy(),
+        g_x=x.grad.numpy(), g_y=y.grad.numpy(), g_r=rr.grad.numpy(), g_theta=tt.grad.numpy(),
+        g_v=vv.grad.numpy(), g_c=cc.grad.numpy())
+    print(f"torch_{name}: N={N} image sum={float(img.sum()):.4f}")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("DIFFBMP_REFERENCE", "/root/reference"))
+    args = ap.parse_args()
+    str_ = load_reference(args.reference)
+    from diffbmp_b200 import workloads as wl
+    import torch
+
+    # template bboxes: soft disk, random shapes, an empty and a one-texel template
+    rng = np.random.default_rng(11)
+    shapes = [wl.soft_disk(64, 24.0), wl.random_shape(rng, 64), wl.random_shape(rng, 64),
+              np.zeros((64, 64), np.float32)]
+    one = np.zeros((64, 64), np.float32); one[7, 50] = 0.5
+    shapes.append(one)
+    edge = np.zeros((64, 64), np.float32); edge[:, 0] = 1e-6; edge[0, :] = 2e-6
+    shapes.append(edge)
+    S = np.stack(shapes)
+    R = make_renderer(str_, 64, 64, S, 32, 1.0)
+    np.savez_compressed(os.path.join(HERE, "tmpl_bbox.npz"), S=S,
+                        bboxes=np.array(R.primitive_bboxes, np.float32))
+    print("tmpl_bbox:", R.primitive_bboxes)
+
+    disk64 = wl.soft_disk(64, 24.0)[None]
+    rng = np.random.default_rng(5)
+    atlas3 = np.stack([wl.random_shape(rng, 48) for _ in range(3)])
+    gen_bin_case(str_, "c0", 256, 256, 32, disk64, 512, 1, 0.05 * 256, 0.3 * 256)
+    gen_bin_case(str_, "ragged", 200, 136, 16, atlas3, 300, 2, 3.0, 60.0, off_canvas=0.2)
+
+    def special(m, r, th):
+        m[0] = (-500.0, -500.0); r[0] = 3.0             # far off canvas
+        m[1] = (64.0, 32.0); r[1] = 1e-7                 # degenerate radius
+        m[2] = (100.0, 100.0); r[2] = 5000.0             # covers everything
+        m[3] = (32.0, 32.0); th[3] = np.float32(np.pi / 2)
+        m[4] = (31.999998, 95.5); r[4] = 0.5; th[4] = 0.0
+    gen_bin_case(str_, "edges", 128, 160, 32, disk64, 64, 3, 2.0, 40.0, special=special)
+
+    rng = np.random.default_rng(9)
+    gen_torch_case(str_, "disk64", 64, 64, 32, wl.soft_disk(32, 12.0)[None], 32, 21, 4.0, 20.0, 1.0)
+    atlas_ns = np.stack([wl.random_shape(rng, 40)[:24, :] for _ in range(3)])  # 24x40, non-square
+    gen_torch_case(str_, "ragged", 80, 96, 16, atlas_ns, 48, 22, 3.0, 25.0, 0.8)
+    torch.set_num_threads(1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,191 @@
+"""GPU parity tests of the sm_100a kernels (called through libdbmp.so).
+
+Bars (stated per test):
+* tile lists and their order: bit-exact;
+* FP32 image / alpha: max-abs <= 1e-5 against the FP64 oracle, except on
+  pixels inside the oracle's boundary band (a fragment within 1e-3 px/texel
+  of the square cull or the texel cut, where float rounding legitimately
+  flips it), which must stay within the band's own spread + 1e-5;
+* gradients: per parameter block ||ours - oracle|| <= 1e-4 ||oracle|| plus
+  the band spread of the gradient.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import binning_torch as BT
+from oracle import oracle as O
+from helpers import bin_scene, golden, rel_err, small_scene, split_mapping
+
+pytestmark = pytest.mark.gpu
+
+R = pytest.importorskip("diffbmp_b200.rasterizer")
+
+
+def dev(sc: O.Scene):
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    return dict(means2D=t(sc.means2D), radii=t(sc.radii), rotations=t(sc.rot), opacities=t(sc.opac),
+                colors=t(sc.colors), sel=torch.from_numpy(sc.sel.astype(np.int32)).cuda(),
+                templates=t(sc.templates))
+
+
+def ours_forward(sc, kind="f32", mapping=None, t_stop=1e-7, bin_mode=R.BIN_CONTENT):
+    d = dev(sc)
+    rz = R.Rasterizer(sc.H, sc.W, sc.ts, sc.alpha_max, t_stop, bin_mode)
+    atlas = R.Atlas(d["templates"], kind)
+    mp = None if mapping is None else torch.from_numpy(mapping).cuda()
+    color, alpha, state = rz.forward(d["means2D"], d["radii"], d["rotations"], d["opacities"], d["colors"],
+                                     d["sel"], atlas, mp)
+    torch.cuda.synchronize()
+    return color.cpu().numpy(), alpha.cpu().numpy(), state, rz, atlas, d
+
+
+def check_image(sc, offs, idx, color, alpha, tol=1e-5):
+    ref = O.forward(sc, offs, idx)
+    band_c, band_a = O.boundary_band(sc, offs, idx, edge=1e-3)
+    ec = np.abs(color - ref["color"]).max(-1)
+    ea = np.abs(alpha - ref["alpha"])
+    sens = (band_c > 0) | (band_a > 0)
+    assert ec[~sens].max(initial=0) <= tol, ("color", ec[~sens].max(initial=0))
+    assert ea[~sens].max(initial=0) <= tol, ("alpha", ea[~sens].max(initial=0))
+    assert np.all(ec[sens] <= band_c[sens] + tol)
+    assert np.all(ea[sens] <= band_a[sens] + tol)
+    return dict(max_err=float(max(ec[~sens].max(initial=0), ea[~sens].max(initial=0))),
+                sensitive=int(sens.sum()), ref=ref)
+
+
+def check_grads(sc, offs, idx, gc, ga, ours, rel=1e-4):
+    """Per block: ||ours - oracle|| <= rel*||oracle|| + ||oracle(+edge) - oracle(-edge)||."""
+    ref = O.backward(sc, offs, idx, gc, ga)
+    hi = O.backward(sc, offs, idx, gc, ga, edge=1e-3)
+    lo = O.backward(sc, offs, idx, gc, ga, edge=-1e-3)
+    for k in range(8):
+        spread = np.linalg.norm(hi[:, k] - lo[:, k])
+        err = np.linalg.norm(ours[:, k] - ref[:, k])
+        nrm = np.linalg.norm(ref[:, k])
+        print(f"  block {k}: err {err:.3e} |ref| {nrm:.3e} band {spread:.3e}")
+        assert err <= rel * nrm + spread + 1e-9, (k, err, nrm, spread)
+
+
+# ---------------------------------------------------------------------------
+# binning
+def test_template_bboxes_gpu():
+    d = golden("tmpl_bbox")
+    atlas = R.Atlas(torch.from_numpy(d["S"]).cuda())
+    assert np.array_equal(atlas.bbox.cpu().numpy(), d["bboxes"])
+
+
+@pytest.mark.parametrize("case", ["c0", "ragged", "edges"])
+def test_binning_matches_reference_gpu(case):
+    d = golden(f"bin_{case}")
+    S = d["S"]
+    N, P = d["radii"].shape[0], S.shape[0]
+    sel = ((N - 1 - np.arange(N)) % P).astype(np.int32)
+    H, W, ts = int(d["H"]), int(d["W"]), int(d["ts"])
+    sc = O.Scene(H, W, ts, d["means2D"], d["radii"], d["rotations"], np.zeros(N), np.zeros((N, 3)), S, sel)
+    dv = dev(sc)
+    rz = R.Rasterizer(H, W, ts)
+    atlas = R.Atlas(dv["templates"])
+    _, lists = rz.bin(dv["means2D"], dv["radii"], dv["rotations"], dv["opacities"], dv["colors"], dv["sel"], atlas)
+    ours = lists.mapping_tensor().cpu().numpy()
+    # the reference binning re-run with torch on this GPU
+    ref_gpu = BT.mapping(H, W, ts, dv["means2D"], dv["radii"], dv["rotations"], atlas.bbox, dv["sel"]).cpu().numpy()
+    assert np.array_equal(ours, ref_gpu)
+    # and the reference's own output (torch on CPU) stored in the fixture
+    assert np.array_equal(ours, d["mapping"])
+
+
+@pytest.mark.parametrize("H,W,ts,N,seed", [(256, 256, 32, 512, 0), (200, 136, 16, 300, 1), (1024, 768, 32, 3000, 2),
+                                           (64, 64, 16, 1, 3), (100, 300, 32, 0, 4)])
+def test_binning_random_gpu(H, W, ts, N, seed):
+    sc = small_scene(seed, H=H, W=W, N=N, P=3, size=48, ts=ts, rmin=1.0, rmax=0.3 * min(H, W))
+    dv = dev(sc)
+    rz = R.Rasterizer(H, W, ts)
+    atlas = R.Atlas(dv["templates"])
+    _, lists = rz.bin(dv["means2D"], dv["radii"], dv["rotations"], dv["opacities"], dv["colors"], dv["sel"], atlas)
+    ref = BT.mapping(H, W, ts, dv["means2D"], dv["radii"], dv["rotations"], atlas.bbox, dv["sel"])
+    assert torch.equal(lists.mapping_tensor(), ref)
+    # cull-square mode against the oracle's exact float predicate
+    rzc = R.Rasterizer(H, W, ts, bin_mode=R.BIN_CULL)
+    _, lc = rzc.bin(dv["means2D"], dv["radii"], dv["rotations"], dv["opacities"], dv["colors"], dv["sel"], atlas)
+    offs, idx = bin_scene(sc, O.BIN_CULL)
+    assert np.array_equal(lc.mapping_tensor().cpu().numpy(), O.mapping_tensor(offs, idx))
+
+
+# ---------------------------------------------------------------------------
+# forward / backward
+SCENES = {
+    "c0": lambda: _spec_scene("c0", 0),
+    "atlas128": lambda: _spec_scene("c1", 1, H=256, W=256, N=800),
+    "ragged16": lambda: small_scene(5, H=200, W=136, N=150, P=3, size=48, ts=16, rmin=3, rmax=50),
+    "nonsquare": lambda: small_scene(6, H=120, W=90, N=60, P=2, size=40, ts=32, nonsquare=True, amax=0.8),
+}
+
+
+def _spec_scene(cfg, seed, **over):
+    from diffbmp_b200 import workloads as wl
+    s = wl.make_scene(cfg, seed, **over)
+    return O.Scene(s.H, s.W, 32, s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.templates, s.sel,
+                   s.alpha_max)
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_forward_parity_gpu(name):
+    sc = SCENES[name]()
+    offs, idx = bin_scene(sc)
+    color, alpha, state, *_ = ours_forward(sc)
+    r = check_image(sc, offs, idx, color, alpha)
+    # per-pixel last contributor never exceeds the oracle's fragment list
+    assert state.last_pos.max().item() < max(len(idx), 1)
+    print(name, r["max_err"], r["sensitive"])
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_backward_parity_gpu(name):
+    sc = SCENES[name]()
+    offs, idx = bin_scene(sc)
+    color, alpha, state, rz, atlas, d = ours_forward(sc)
+    rng = np.random.default_rng(7)
+    gc = rng.normal(0, 1, (sc.H, sc.W, 3)).astype(np.float32)
+    ga = rng.normal(0, 1, (sc.H, sc.W)).astype(np.float32)
+    grads = rz.backward(state, torch.from_numpy(gc).cuda(), torch.from_numpy(ga).cuda(), d["radii"],
+                        d["rotations"], d["opacities"], d["colors"], atlas)
+    ours = np.concatenate([g.cpu().numpy().reshape(sc.N, -1) for g in grads], 1)
+    check_grads(sc, offs, idx, gc, ga, ours)
+
+
+def test_caller_mapping_equals_device_binning_gpu():
+    """A caller-supplied reference mapping and the device binning render the same image."""
+    sc = SCENES["atlas128"]()
+    offs, idx = bin_scene(sc)
+    c1, a1, *_ = ours_forward(sc)
+    c2, a2, *_ = ours_forward(sc, mapping=O.mapping_tensor(offs, idx))
+    assert np.array_equal(c1, c2) and np.array_equal(a1, a2)
+
+
+def test_autograd_function_gpu():
+    sc = SCENES["c0"]()
+    d = dev(sc)
+    rz = R.Rasterizer(sc.H, sc.W, sc.ts)
+    atlas = R.Atlas(d["templates"])
+    params = [d[k].clone().requires_grad_(True) for k in ("means2D", "radii", "rotations", "opacities", "colors")]
+    color, alpha = R.rasterize(*params, d["sel"], atlas, rz)
+    rng = np.random.default_rng(3)
+    wc = torch.from_numpy(rng.normal(0, 1, (sc.H, sc.W, 3)).astype(np.float32)).cuda()
+    wa = torch.from_numpy(rng.normal(0, 1, (sc.H, sc.W)).astype(np.float32)).cuda()
+    ((color * wc).sum() + (alpha * wa).sum()).backward()
+    offs, idx = bin_scene(sc)
+    ours = np.concatenate([p.grad.cpu().numpy().reshape(sc.N, -1) for p in params], 1)
+    check_grads(sc, offs, idx, wc.cpu().numpy(), wa.cpu().numpy(), ours)
+
+
+@pytest.mark.parametrize("kind,min_psnr", [("f32q", 90.0), ("f16", 60.0), ("bf16", 45.0)])
+def test_precision_forms_gpu(kind, min_psnr):
+    sc = SCENES["atlas128"]()
+    offs, idx = bin_scene(sc)
+    color, alpha, *_ = ours_forward(sc, kind=kind)
+    ref = O.forward(sc, offs, idx)
+    mse = float(np.mean((color - ref["color"]) ** 2))
+    psnr = 10 * np.log10(1.0 / max(mse, 1e-30))
+    print(kind, "PSNR", psnr, "max", np.abs(color - ref["color"]).max())
+    assert psnr >= min_psnr
