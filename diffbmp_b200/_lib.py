@@ -21,6 +21,13 @@ BIN_CONTENT, BIN_CULL = 0, 1
 _vp, _i, _ll, _sz, _f = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_size_t, ctypes.c_float
 
 
+class AdamCfg(ctypes.Structure):
+    """Mirror of dbmp_adam_cfg."""
+    _fields_ = [("lr", ctypes.c_float * 8), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("eps", ctypes.c_float), ("x_max", ctypes.c_float), ("y_max", ctypes.c_float),
+                ("r_min", ctypes.c_float), ("r_max", ctypes.c_float), ("clamp", ctypes.c_int32)]
+
+
 class Canvas(ctypes.Structure):
     """Mirror of dbmp_canvas."""
     _fields_ = [("height", ctypes.c_int32), ("width", ctypes.c_int32), ("tile_size", ctypes.c_int32),
@@ -44,6 +51,9 @@ SIGNATURES = {
     "dbmp_forward": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_backward": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                            _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_count": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_fused_fwd_bwd": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_adam_step": (_i, [_CP, ctypes.c_void_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 

@@ -33,6 +33,8 @@ int launch_bin(const Geom& g, int bin_mode, const float* means2D, const float* r
                void* ws, size_t ws_bytes, cudaStream_t st);
 int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                    const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st);
+int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
+                 unsigned long long* cnt, cudaStream_t st);
 int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                     const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
                     const float* grad_alpha, double* gacc, cudaStream_t st);
@@ -40,7 +42,16 @@ int launch_finalize(const Geom& g, const float* radii, const float* rot, const f
                     const double* gacc, float* gm, float* gr, float* grot, float* go, float* gc, cudaStream_t st);
 int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  const float* target, const float* background, float* out_image, double* gacc, double* loss,
-                 cudaStream_t st);
+                 const int* skip_flag, cudaStream_t st);
+struct AdamArgs {
+  float lr[8];
+  float beta1, beta2, eps;
+  float x_max, y_max, r_min, r_max;
+  int clamp;
+};
+int launch_adam(const Geom& g, const AdamArgs& a, const double* gacc, float* means2D, float* radii, float* rot,
+                float* opac, float* colors, float* m1, float* m2, int* step_count, const int* skip_flag,
+                cudaStream_t st);
 
 // Validates a canvas description and derives the launch geometry.
 int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
@@ -176,6 +187,55 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
   if (rc) return rc;
   return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
                          grad_rotations, grad_opacities, grad_colors, st);
+}
+
+int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
+               const int32_t* tile_indices, unsigned long long* counts, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_count");
+  if (rc) return rc;
+  REQUIRE(atlas && tile_offsets && tile_indices && counts, "dbmp_count: null pointer");
+  REQUIRE(g.N == 0 || prim_info, "dbmp_count: prim_info is null");
+  cudaError_t e = cudaMemsetAsync(counts, 0, 3 * sizeof(unsigned long long), (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(counts)");
+  return launch_count(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, counts,
+                      (cudaStream_t)stream);
+}
+
+int dbmp_fused_fwd_bwd(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
+                       const int32_t* tile_indices, const float* target, const float* background, float* out_image,
+                       double* grad_accum, double* loss_out, const int32_t* skip_flag, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_fused_fwd_bwd");
+  if (rc) return rc;
+  REQUIRE(atlas && tile_offsets && tile_indices && target && loss_out, "dbmp_fused_fwd_bwd: null input");
+  REQUIRE(g.N == 0 || (prim_info && grad_accum), "dbmp_fused_fwd_bwd: null prim_info / grad_accum");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(loss_out, 0, sizeof(double), st);
+  if (e == cudaSuccess && g.N > 0) e = cudaMemsetAsync(grad_accum, 0, sizeof(double) * 8 * (size_t)g.N, st);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(fused outputs)");
+  return launch_fused(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, target,
+                      background, out_image, grad_accum, loss_out, skip_flag, st);
+}
+
+int dbmp_adam_step(const dbmp_canvas* cv, const dbmp_adam_cfg* cfg, const double* grad_accum, float* means2D,
+                   float* radii, float* rotations, float* opacities, float* colors, float* adam_m, float* adam_v,
+                   int32_t* step_count, const int32_t* skip_flag, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_adam_step");
+  if (rc) return rc;
+  REQUIRE(cfg && step_count, "dbmp_adam_step: null cfg / step_count");
+  REQUIRE(g.N == 0 || (grad_accum && means2D && radii && rotations && opacities && colors && adam_m && adam_v),
+          "dbmp_adam_step: null pointer");
+  REQUIRE(cfg->beta1 >= 0.f && cfg->beta1 < 1.f && cfg->beta2 >= 0.f && cfg->beta2 < 1.f && cfg->eps > 0.f,
+          "dbmp_adam_step: betas must be in [0,1) and eps > 0");
+  AdamArgs a;
+  for (int k = 0; k < 8; ++k) a.lr[k] = cfg->lr[k];
+  a.beta1 = cfg->beta1; a.beta2 = cfg->beta2; a.eps = cfg->eps;
+  a.x_max = cfg->x_max; a.y_max = cfg->y_max; a.r_min = cfg->r_min; a.r_max = cfg->r_max;
+  a.clamp = cfg->clamp;
+  return launch_adam(g, a, grad_accum, means2D, radii, rotations, opacities, colors, adam_m, adam_v, step_count,
+                     skip_flag, (cudaStream_t)stream);
 }
 
 }  // extern "C"

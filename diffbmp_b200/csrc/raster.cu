@@ -86,10 +86,15 @@ struct TileWalker {
     fy1 = fy0 + (float)(L::FH - 1);
   }
 
+  // STATS: count (pixel, primitive) pairs that pass the cull and fragments
+  // composited, both before termination, into cnt[0], cnt[1].
+  template <bool STATS = false>
   __device__ __forceinline__ void forward(const Geom& g, const PrimInfo* __restrict__ prims,
                                           const void* __restrict__ atlas, const int* __restrict__ idx,
                                           float4 (*s_pi)[4], int* s_id,
-                                          float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP]) {
+                                          float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP],
+                                          unsigned long long* cnt = nullptr) {
+    unsigned long long n_cand = 0, n_frag = 0;
     bool done[NP];
     bool all_done = true;
 #pragma unroll
@@ -122,7 +127,9 @@ struct TileWalker {
                 const float tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
                 const float ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
                 const float m = sample_mask<KIND, false>(atlas, tmpl, g.Ht, g.Wt, tx, ty, nullptr, nullptr);
+                if (STATS) ++n_cand;
                 if (m > 1e-6f) {
+                  if (STATS) ++n_frag;
                   const float a = g2.x * m;
                   const float w = T[p] * a;
                   C[p][0] = fmaf(w, g2.y, C[p][0]);
@@ -141,6 +148,10 @@ struct TileWalker {
         }
       }
       if (__syncthreads_and(warp_done)) break;
+    }
+    if (STATS) {
+      atomicAdd(cnt + 0, n_cand);
+      atomicAdd(cnt + 1, n_frag);
     }
   }
 
@@ -294,6 +305,24 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(Geom g, const PrimInf
   }
 }
 
+// Counting pass (diagnostics / roofline accounting): same walk as the
+// forward, no outputs except the counters.
+template <int TS, int KIND>
+__global__ void __launch_bounds__(kThreads) count_kernel(Geom g, const PrimInfo* __restrict__ prims,
+                                                         const void* __restrict__ atlas,
+                                                         const int* __restrict__ offs, const int* __restrict__ idx,
+                                                         unsigned long long* __restrict__ cnt) {
+  __shared__ float4 s_pi[kChunk][4];
+  __shared__ int s_id[kChunk];
+  TileWalker<TS, KIND> tw;
+  tw.init(g, blockIdx.x, offs);
+  constexpr int NP = TileWalker<TS, KIND>::NP;
+  float C[NP][3], T[NP], Tl[NP];
+  int lp[NP];
+  tw.template forward<true>(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp, cnt);
+  if (threadIdx.x == 0) atomicAdd(cnt + 2, (unsigned long long)(tw.end - tw.start));
+}
+
 template <int TS, int KIND>
 __global__ void __launch_bounds__(kThreads) backward_kernel(Geom g, const PrimInfo* __restrict__ prims,
                                                             const void* __restrict__ atlas,
@@ -378,7 +407,9 @@ __global__ void __launch_bounds__(kThreads) fused_kernel(Geom g, const PrimInfo*
                                                          const float* __restrict__ target,
                                                          const float* __restrict__ background,
                                                          float* __restrict__ out_image, double* __restrict__ gacc,
-                                                         double* __restrict__ loss_out) {
+                                                         double* __restrict__ loss_out,
+                                                         const int* __restrict__ skip_flag) {
+  if (skip_flag != nullptr && *skip_flag != 0) return;   // binning overflowed: leave all state untouched
   __shared__ float4 s_pi[kChunk][4];
   __shared__ int s_id[kChunk];
   __shared__ float s_part[kThreads / 32][kChunk][8];
@@ -450,6 +481,15 @@ int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* a
   return DBMP_OK;
 }
 
+int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
+                 unsigned long long* cnt, cudaStream_t st) {
+  if (g.T == 0) return DBMP_OK;
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (count_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+                                                   g, prims, atlas, offs, idx, cnt))));
+  DBMP_CHECK_LAUNCH("count_kernel");
+  return DBMP_OK;
+}
+
 int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                     const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
                     const float* grad_alpha, double* gacc, cudaStream_t st) {
@@ -471,11 +511,11 @@ int launch_finalize(const Geom& g, const float* radii, const float* rot, const f
 
 int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  const float* target, const float* background, float* out_image, double* gacc, double* loss,
-                 cudaStream_t st) {
+                 const int* skip_flag, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
   DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (fused_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
                                                    g, prims, atlas, offs, idx, target, background, out_image,
-                                                   gacc, loss))));
+                                                   gacc, loss, skip_flag))));
   DBMP_CHECK_LAUNCH("fused_kernel");
   return DBMP_OK;
 }

@@ -143,6 +143,54 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
                   float* grad_means2D, float* grad_radii, float* grad_rotations,
                   float* grad_opacities, float* grad_colors, void* stream);
 
+/* Counting pass over the same walk as dbmp_forward (no image output):
+ * counts[0] = (pixel, primitive) pairs that pass the square cull before the
+ * pixel terminates, counts[1] = fragments composited, counts[2] = tile-list
+ * entries (sum over tiles).  counts: 3 device u64, zeroed by the call.  Used
+ * for roofline accounting; no reference counterpart. */
+int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+               const int32_t* tile_offsets, const int32_t* tile_indices,
+               unsigned long long* counts, void* stream);
+
+/* Fused forward + L2 loss + backward of one image-fitting iteration, one
+ * CTA per tile: the forward walk composites, the CTA forms the reference
+ * loss gradient of rendered = C + (1-A)*background against `target`
+ * (mse_loss, pydiffbmp/util/loss_functions.py:20-40 on
+ * simple_tile_renderer.py:704-707) and walks the same list back.  Zeroes and
+ * fills grad_accum ((N,8) f64 raw per-primitive sums, consumed by
+ * dbmp_adam_step) and *loss_out (device f64, mean squared error).
+ * target / background (H,W,3) f32; background may be null (black);
+ * out_image (H,W,3) f32 may be null.  If skip_flag (device int32, may be
+ * null) is non-zero the call leaves every output untouched (used with
+ * dbmp_bin's overflow flag).  Replaces the sequence forward kernel -> torch
+ * loss -> backward kernel of simple_tile_renderer.py:1059-1074. */
+int dbmp_fused_fwd_bwd(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+                       const int32_t* tile_offsets, const int32_t* tile_indices,
+                       const float* target, const float* background, float* out_image,
+                       double* grad_accum, double* loss_out, const int32_t* skip_flag,
+                       void* stream);
+
+/* Optimiser settings of dbmp_adam_step: learning rate per parameter in the
+ * order x, y, r, theta, opacity, colour r/g/b; Adam betas/eps; clamp bounds. */
+typedef struct {
+  float lr[8];
+  float beta1, beta2, eps;
+  float x_max, y_max, r_min, r_max;
+  int32_t clamp;          /* 1: clamp x, y, r after the step */
+} dbmp_adam_cfg;
+
+/* In-place Adam step of every primitive parameter from the raw sums in
+ * grad_accum (as left by dbmp_fused_fwd_bwd or dbmp_backward), followed by
+ * the reference's parameter clamp.  adam_m / adam_v: (N,8) f32 moments;
+ * step_count: device int32 of completed steps (incremented here).  If
+ * skip_flag is non-zero nothing changes.  Replaces torch.optim.Adam.step +
+ * _clamp_params_inplace (pydiffbmp/core/renderer/simple_tile_renderer.py:961-968,
+ * 1125-1131, 122-128). */
+int dbmp_adam_step(const dbmp_canvas* cv, const dbmp_adam_cfg* cfg, const double* grad_accum,
+                   float* means2D, float* radii, float* rotations, float* opacities, float* colors,
+                   float* adam_m, float* adam_v, int32_t* step_count, const int32_t* skip_flag,
+                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif
