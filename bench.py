@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c0", "c1", "c2"])
     ap.add_argument("--fast", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--profile", default=None, choices=["f16", "f32", "bf16", "f32q", "f16q", "bf16q", "plain"],
+                    help="profiling mode: one job of this form, --warmup + --steps eager steps, no timing line")
     return ap.parse_args()
 
 
@@ -276,6 +278,15 @@ def main():
     rank, world, local = dist_setup(args)
     from diffbmp_b200 import workloads as wl
     spec = wl.make_scene(args.config, seed=rank)
+    if args.profile:
+        kind = "f32" if args.profile == "plain" else args.profile
+        job = build_job(spec, kind, args.profile != "plain", torch)
+        for _ in range(args.warmup + args.steps):
+            job.step()
+        job.sync()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "steps": args.warmup + args.steps, "loss": job.loss()}))
+        return
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))

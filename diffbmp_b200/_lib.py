@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdbmp.so")
 
 DBMP_OK, DBMP_ERR_INVALID, DBMP_ERR_CUDA, DBMP_ERR_CAPACITY, DBMP_ERR_UNSUPPORTED = range(5)
-ATLAS_F32, ATLAS_F32_QUAD, ATLAS_F16_QUAD, ATLAS_BF16_QUAD = range(4)
+ATLAS_F32, ATLAS_F32_QUAD, ATLAS_F16_QUAD, ATLAS_BF16_QUAD, ATLAS_F16_PAIR, ATLAS_BF16_PAIR = range(6)
 BIN_CONTENT, BIN_CULL = 0, 1
 
 # Every symbol include/dbmp.h declares, with (restype, argtypes).
@@ -44,6 +44,7 @@ SIGNATURES = {
     "dbmp_num_tiles": (_i, [_CP]),
     "dbmp_template_bboxes": (_i, [_vp, _i, _i, _i, _vp, _vp]),
     "dbmp_atlas_pack": (_i, [_vp, _i, _i, _i, _i, _vp, _vp]),
+    "dbmp_atlas_bytes": (_sz, [_i, _i, _i, _i]),
     "dbmp_bin_workspace_bytes": (_sz, [_CP, _ll]),
     "dbmp_prim_info_bytes": (_sz, [_i]),
     "dbmp_prepare": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

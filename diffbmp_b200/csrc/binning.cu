@@ -54,6 +54,22 @@ template <> __device__ __forceinline__ float to_storage<float>(float v) { return
 template <> __device__ __forceinline__ __half to_storage<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 to_storage<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
+// Pair layout: (P, Ht+1, Wt) records of (t[y][x], t[y][x+1]); row Ht is zero.
+template <typename OutT>
+__global__ void atlas_pair_kernel(const float* __restrict__ tmpl, int P, int Ht, int Wt, OutT* __restrict__ out) {
+  const long long total = (long long)P * (Ht + 1) * Wt;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % Wt);
+    const int y = (int)((i / Wt) % (Ht + 1));
+    const long long p = i / ((long long)(Ht + 1) * Wt);
+    const float* t = tmpl + (size_t)p * Ht * Wt;
+    const float v0 = (y < Ht) ? t[(size_t)y * Wt + x] : 0.f;
+    const float v1 = (y < Ht && x + 1 < Wt) ? t[(size_t)y * Wt + x + 1] : 0.f;
+    out[2 * i] = to_storage<OutT>(v0);
+    out[2 * i + 1] = to_storage<OutT>(v1);
+  }
+}
+
 template <typename OutT>
 __global__ void atlas_pack_kernel(const float* __restrict__ tmpl, int P, int Ht, int Wt, OutT* __restrict__ out) {
   const long long total = (long long)P * Ht * Wt;
@@ -148,7 +164,8 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
   pi.cr = sigmoid_precise(colors[3 * n + 0]);
   pi.cg = sigmoid_precise(colors[3 * n + 1]);
   pi.cb = sigmoid_precise(colors[3 * n + 2]);
-  pi.tmpl = valid ? tid : -1;
+  const bool nan_geom = isnan(pi.a00) || isnan(pi.a01) || isnan(pi.a10) || isnan(pi.a11) || isnan(mx) || isnan(my);
+  pi.toff = !valid ? kNoFrag : (nan_geom ? kSolid : tid * template_records(g.kind, g.Ht, g.Wt));
   pi.rinv = (float)rinv; pi.cs = (float)c; pi.sn = (float)s;
   out[n] = pi;
 
@@ -299,11 +316,24 @@ int launch_template_bboxes(const float* tmpl, int P, int Ht, int Wt, float* out,
   return DBMP_OK;
 }
 
+size_t atlas_bytes(int P, int Ht, int Wt, int kind) {
+  const size_t recs = (size_t)P * template_records(kind, Ht, Wt);
+  switch (kind) {
+    case ATLAS_F32: return recs * 4;
+    case ATLAS_F32_QUAD: return recs * 16;
+    case ATLAS_F16_QUAD: case ATLAS_BF16_QUAD: return recs * 8;
+    case ATLAS_F16_PAIR: case ATLAS_BF16_PAIR: return recs * 4;
+    default: return 0;
+  }
+}
+
 int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st) {
-  const long long total = (long long)P * Ht * Wt;
+  const long long total = (long long)P * (Ht + 1) * Wt;
   if (total == 0) return DBMP_OK;
   const int blocks = (int)((total + 255) / 256 < 148 * 32 ? (total + 255) / 256 : 148 * 32);
   switch (kind) {
+    case ATLAS_F16_PAIR: atlas_pair_kernel<__half><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (__half*)out); break;
+    case ATLAS_BF16_PAIR: atlas_pair_kernel<__nv_bfloat16><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (__nv_bfloat16*)out); break;
     case ATLAS_F32_QUAD: atlas_pack_kernel<float><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (float*)out); break;
     case ATLAS_F16_QUAD: atlas_pack_kernel<__half><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (__half*)out); break;
     case ATLAS_BF16_QUAD: atlas_pack_kernel<__nv_bfloat16><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (__nv_bfloat16*)out); break;

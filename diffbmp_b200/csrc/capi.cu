@@ -23,6 +23,7 @@ int cuda_status(cudaError_t e, const char* what) {
 
 // launchers (binning.cu, raster.cu)
 size_t bin_workspace_bytes(int N, int T, long long cap);
+size_t atlas_bytes(int P, int Ht, int Wt, int kind);
 int launch_template_bboxes(const float* tmpl, int P, int Ht, int Wt, float* out, cudaStream_t st);
 int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st);
 int launch_prepare(const Geom& g, const float* means2D, const float* radii, const float* rot, const float* opac,
@@ -63,7 +64,7 @@ int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
     set_error("%s: template atlas %dx%dx%d is invalid (need P>=1, Ht,Wt>=2)", who, cv->num_templates, cv->tmpl_h, cv->tmpl_w);
     return DBMP_ERR_INVALID;
   }
-  if (cv->atlas_kind < DBMP_ATLAS_F32 || cv->atlas_kind > DBMP_ATLAS_BF16_QUAD) { set_error("%s: atlas_kind %d unknown", who, cv->atlas_kind); return DBMP_ERR_INVALID; }
+  if (cv->atlas_kind < DBMP_ATLAS_F32 || cv->atlas_kind > DBMP_ATLAS_BF16_PAIR) { set_error("%s: atlas_kind %d unknown", who, cv->atlas_kind); return DBMP_ERR_INVALID; }
   if (!(cv->t_stop >= 1e-30f && cv->t_stop < 1.f)) { set_error("%s: t_stop %g outside [1e-30, 1)", who, (double)cv->t_stop); return DBMP_ERR_INVALID; }
   if ((long long)cv->height * cv->width > (1ll << 31) / 4) { set_error("%s: canvas too large", who); return DBMP_ERR_INVALID; }
   g->H = cv->height; g->W = cv->width; g->TS = cv->tile_size;
@@ -75,6 +76,9 @@ int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
   g->hy = 0.5f * (float)(cv->tmpl_h - 1);
   g->rxy = g->hx / g->hy;
   g->ryx = g->hy / g->hx;
+  g->wm1 = (float)(cv->tmpl_w - 1);
+  g->hm1 = (float)(cv->tmpl_h - 1);
+  g->kind = cv->atlas_kind;
   g->alpha_max = cv->alpha_max;
   g->t_stop = cv->t_stop;
   return DBMP_OK;
@@ -110,6 +114,11 @@ int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, voi
   REQUIRE(P >= 0 && Ht >= 1 && Wt >= 1, "dbmp_atlas_pack: bad atlas shape %dx%dx%d", P, Ht, Wt);
   REQUIRE(P == 0 || (templates && out), "dbmp_atlas_pack: null pointer");
   return launch_atlas_pack(templates, P, Ht, Wt, kind, out, (cudaStream_t)stream);
+}
+
+size_t dbmp_atlas_bytes(int P, int Ht, int Wt, int kind) {
+  if (P < 0 || Ht < 1 || Wt < 1) return 0;
+  return atlas_bytes(P, Ht, Wt, kind);
 }
 
 size_t dbmp_bin_workspace_bytes(const dbmp_canvas* cv, long long capacity) {

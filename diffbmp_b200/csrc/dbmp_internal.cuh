@@ -21,37 +21,54 @@ struct __align__(16) PrimInfo {
   float mx, my, hw, hh;      // centre, square-cull half extents (tile_forward.cu:194-210)
   float a00, a01, a10, a11;  // inverse affine to texel coordinates
   float alpha0, cr, cg, cb;  // alpha_max*sigmoid(opacity), sigmoid(colour logits)
-  int tmpl;                  // template id, -1 when the primitive yields no fragments
-  float rinv, cs, sn;        // reference r_inv and rotation cos/sin (backward chain)
+  int toff;                  // first element of the template in the atlas; kNoFrag / kSolid
+  float rinv, cs, sn;        // reference r_inv and rotation cos/sin
 };
 static_assert(sizeof(PrimInfo) == 64, "PrimInfo must be 64 bytes");
 
+// toff sentinels.  kNoFrag: invalid template id, the primitive never yields a
+// fragment (tile_forward.cu:211-216,274).  kSolid: NaN geometry; the
+// reference's range test lets NaN texel coordinates through, reads texel 0
+// and clamps the NaN mask to 1 (tile_common.h:177-197 + tile_forward.cu:271),
+// i.e. the primitive is opaque-by-mask wherever its cull passes.
+constexpr int kNoFrag = -1;
+constexpr int kSolid = -2;
+
 // Texel storage of the template atlas.
 enum AtlasKind : int {
-  ATLAS_F32 = DBMP_ATLAS_F32,            // (P,Ht,Wt) float32, the reference layout
-  ATLAS_F32_QUAD = DBMP_ATLAS_F32_QUAD,  // (P,Ht,Wt) x 4 float32 bilinear quads
-  ATLAS_F16_QUAD = DBMP_ATLAS_F16_QUAD,  // (P,Ht,Wt) x 4 half
-  ATLAS_BF16_QUAD = DBMP_ATLAS_BF16_QUAD // (P,Ht,Wt) x 4 bfloat16
+  ATLAS_F32 = DBMP_ATLAS_F32,              // (P,Ht,Wt) float32, the reference layout
+  ATLAS_F32_QUAD = DBMP_ATLAS_F32_QUAD,    // (P,Ht,Wt) x 4 float32 bilinear quads
+  ATLAS_F16_QUAD = DBMP_ATLAS_F16_QUAD,    // (P,Ht,Wt) x 4 half
+  ATLAS_BF16_QUAD = DBMP_ATLAS_BF16_QUAD,  // (P,Ht,Wt) x 4 bfloat16
+  ATLAS_F16_PAIR = DBMP_ATLAS_F16_PAIR,    // (P,Ht+1,Wt) x 2 half (x, x+1), zero last row
+  ATLAS_BF16_PAIR = DBMP_ATLAS_BF16_PAIR   // (P,Ht+1,Wt) x 2 bfloat16
 };
+
+// Elements (texel records) per template for a storage kind.
+__host__ __device__ inline int template_records(int kind, int Ht, int Wt) {
+  return (kind == ATLAS_F16_PAIR || kind == ATLAS_BF16_PAIR) ? (Ht + 1) * Wt : Ht * Wt;
+}
 
 struct Geom {
   int H, W, TS, tilesX, tilesY, T;
   int N, P, Ht, Wt;
+  int kind;            // AtlasKind of the atlas the kernels read
   float hx, hy;        // (Wt-1)/2, (Ht-1)/2
   float rxy, ryx;      // hx/hy, hy/hx (rotation gradient of non-square templates)
+  float wm1, hm1;      // Wt-1, Ht-1
   float alpha_max;
   float t_stop;
 };
 
-// Quad of bilinear neighbours (v00, v01, v10, v11) of texel (x0, y0); entries
+// Bilinear neighbours (v00, v01, v10, v11) of texel (x0, y0); neighbours
 // outside the template read 0 (tile_common.h:188-194).
 struct Quad { float v00, v01, v10, v11; };
 
 template <int KIND> struct AtlasFetch;
 
 template <> struct AtlasFetch<ATLAS_F32> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int tmpl, int Ht, int Wt, int x0, int y0) {
-    const float* t = static_cast<const float*>(atlas) + (size_t)tmpl * Ht * Wt + (size_t)y0 * Wt + x0;
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const float* t = static_cast<const float*>(atlas) + off + y0 * Wt + x0;
     const bool xr = x0 + 1 < Wt, yr = y0 + 1 < Ht;
     Quad q;
     q.v00 = __ldg(t);
@@ -63,52 +80,79 @@ template <> struct AtlasFetch<ATLAS_F32> {
 };
 
 template <> struct AtlasFetch<ATLAS_F32_QUAD> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int tmpl, int Ht, int Wt, int x0, int y0) {
-    const float4 v = __ldg(static_cast<const float4*>(atlas) + (size_t)tmpl * Ht * Wt + (size_t)y0 * Wt + x0);
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const float4 v = __ldg(static_cast<const float4*>(atlas) + off + y0 * Wt + x0);
     return Quad{v.x, v.y, v.z, v.w};
   }
 };
 
+__device__ __forceinline__ float2 h2f(unsigned u) { return __half22float2(*reinterpret_cast<const __half2*>(&u)); }
+__device__ __forceinline__ float2 b2f(unsigned u) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u));
+}
+
 template <> struct AtlasFetch<ATLAS_F16_QUAD> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int tmpl, int Ht, int Wt, int x0, int y0) {
-    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + (size_t)tmpl * Ht * Wt + (size_t)y0 * Wt + x0);
-    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + off + y0 * Wt + x0);
+    const float2 a = h2f(raw.x), b = h2f(raw.y);
     return Quad{a.x, a.y, b.x, b.y};
   }
 };
 
 template <> struct AtlasFetch<ATLAS_BF16_QUAD> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int tmpl, int Ht, int Wt, int x0, int y0) {
-    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + (size_t)tmpl * Ht * Wt + (size_t)y0 * Wt + x0);
-    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
-    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + off + y0 * Wt + x0);
+    const float2 a = b2f(raw.x), b = b2f(raw.y);
     return Quad{a.x, a.y, b.x, b.y};
   }
 };
 
-// Template mask at texel coordinate (tx, ty): bilinear with a hard zero
-// outside [0,Wt-1]x[0,Ht-1] (tile_common.h:175-198), clamped to [0,1]
-// (tile_forward.cu:271, same operand order).  A NaN coordinate passes the
-// reference's range test, converts to texel 0 and clamps to 1 through
-// fmaxf(0, fminf(1, NaN)); the same happens here.  When GRAD is set also
-// returns d(mask)/d(tex) before the clamp (tile_common.h:201-239).
+template <> struct AtlasFetch<ATLAS_F16_PAIR> {
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const unsigned* p = static_cast<const unsigned*>(atlas) + off + y0 * Wt + x0;
+    const float2 a = h2f(__ldg(p)), b = h2f(__ldg(p + Wt));   // row Ht is the zero pad
+    return Quad{a.x, a.y, b.x, b.y};
+  }
+};
+
+template <> struct AtlasFetch<ATLAS_BF16_PAIR> {
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const unsigned* p = static_cast<const unsigned*>(atlas) + off + y0 * Wt + x0;
+    const float2 a = b2f(__ldg(p)), b = b2f(__ldg(p + Wt));
+    return Quad{a.x, a.y, b.x, b.y};
+  }
+};
+
+// floor(v) for 0 <= v < 2^23 without a float<->int conversion: adding 2^23
+// with round-toward-zero leaves floor(v) in the low mantissa bits.
+__device__ __forceinline__ int floor_small(float v, float* fl) {
+  const float b = __fadd_rz(v, 8388608.f);
+  *fl = b - 8388608.f;
+  return __float_as_int(b) - 0x4B000000;
+}
+
+// Template mask at texel coordinate (tx, ty) of the template starting at
+// `off`: bilinear with a hard zero outside [0,Wt-1]x[0,Ht-1]
+// (tile_common.h:175-198), clamped to [0,1] (tile_forward.cu:271).  NaN
+// coordinates never reach here (kSolid primitives are handled by the caller).
+// With GRAD also returns d(mask)/d(tex) before the clamp (tile_common.h:201-239).
 template <int KIND, bool GRAD>
-__device__ __forceinline__ float sample_mask(const void* atlas, int tmpl, int Ht, int Wt, float tx, float ty,
+__device__ __forceinline__ float sample_mask(const void* atlas, int off, const Geom& g, float tx, float ty,
                                              float* gx, float* gy) {
-  if (tx < 0.f || tx > (float)(Wt - 1) || ty < 0.f || ty > (float)(Ht - 1)) {
+  if (!(tx >= 0.f && tx <= g.wm1 && ty >= 0.f && ty <= g.hm1)) {
     if (GRAD) { *gx = 0.f; *gy = 0.f; }
     return 0.f;
   }
-  // tx, ty in [0, W-1] (or NaN -> 0): truncation is floor and stays in range
-  const int x0 = __float2int_rz(tx), y0 = __float2int_rz(ty);
-  const float wx = tx - (float)x0, wy = ty - (float)y0;
-  const Quad q = AtlasFetch<KIND>::get(atlas, tmpl, Ht, Wt, x0, y0);
-  const float top = fmaf(wx, q.v01 - q.v00, q.v00);
-  const float bot = fmaf(wx, q.v11 - q.v10, q.v10);
+  float fx, fy;
+  const int x0 = floor_small(tx, &fx), y0 = floor_small(ty, &fy);
+  const float wx = tx - fx, wy = ty - fy;
+  const Quad q = AtlasFetch<KIND>::get(atlas, off, g.Ht, g.Wt, x0, y0);
+  const float dt = q.v01 - q.v00, db = q.v11 - q.v10;
+  const float top = fmaf(wx, dt, q.v00);
+  const float bot = fmaf(wx, db, q.v10);
   const float m = fmaf(wy, bot - top, top);
   if (GRAD) {
-    *gx = fmaf(wy, (q.v11 - q.v10) - (q.v01 - q.v00), q.v01 - q.v00);
+    *gx = fmaf(wy, db - dt, dt);
     *gy = bot - top;
   }
   return fmaxf(0.f, fminf(1.f, m));

@@ -38,7 +38,7 @@ __device__ __forceinline__ void stage_chunk(const PrimInfo* __restrict__ prims, 
       v = __ldg(reinterpret_cast<const float4*>(prims + id) + q);
     } else {  // out-of-range ids are skipped like tile_forward.cu:184-185
       v = make_float4(0.f, 0.f, -1.f, -1.f);
-      if (q == 3) v.x = __int_as_float(-1);
+      if (q == 3) v.x = __int_as_float(kNoFrag);
     }
     s_pi[e][q] = v;
     if (q == 0) s_id[e] = (id >= 0 && id < N) ? id : -1;
@@ -51,6 +51,27 @@ __device__ __forceinline__ void stage_chunk(const PrimInfo* __restrict__ prims, 
 __device__ __forceinline__ bool footprint_miss(const float4& g0, float x0, float x1, float y0, float y1) {
   return (g0.x - g0.z > x1 + 1.f) || (g0.x + g0.z < x0 - 1.f) || (g0.y - g0.w > y1 + 1.f) ||
          (g0.y + g0.w < y0 - 1.f);
+}
+
+// Warp-uniform: true when every pixel of the warp footprint passes the
+// primitive's square cull with a 1 px margin, so the per-pixel cull can be
+// skipped (false for NaN geometry, which then takes the per-pixel path).
+__device__ __forceinline__ bool footprint_inside(const float4& g0, float x0, float x1, float y0, float y1) {
+  return (g0.x - g0.z <= x0 - 1.f) && (g0.x + g0.z >= x1 + 1.f) && (g0.y - g0.w <= y0 - 1.f) &&
+         (g0.y + g0.w >= y1 + 1.f);
+}
+
+// Mask of one (pixel, primitive) pair; 0 when the pair yields no fragment.
+template <int KIND, bool GRAD>
+__device__ __forceinline__ float pair_mask(const Geom& g, const void* atlas, int toff, const float4& g1,
+                                           float dx, float dy, float* tx, float* ty, float* gx, float* gy) {
+  *tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
+  *ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
+  if (toff == kSolid) {
+    if (GRAD) { *gx = __int_as_float(0x7fc00000); *gy = *gx; }
+    return 1.f;
+  }
+  return sample_mask<KIND, GRAD>(atlas, toff, g, *tx, *ty, gx, gy);
 }
 
 // ---------------------------------------------------------------------------
@@ -113,8 +134,9 @@ struct TileWalker {
         for (int e = 0; e < n; ++e) {
           const float4 g0 = s_pi[e][0];
           if (footprint_miss(g0, fx0, fx1, fy0, fy1)) continue;
-          const int tmpl = __float_as_int(s_pi[e][3].x);
-          if (tmpl < 0) continue;
+          const int toff = __float_as_int(s_pi[e][3].x);
+          if (toff == kNoFrag) continue;
+          const bool inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
           const float4 g1 = s_pi[e][1];
           const float4 g2 = s_pi[e][2];
           const int pos = base - start + e;
@@ -123,10 +145,9 @@ struct TileWalker {
           for (int p = 0; p < NP; ++p) {
             if (!done[p]) {
               const float dx = (float)px[p] - g0.x, dy = (float)py[p] - g0.y;
-              if (!(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
-                const float tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
-                const float ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
-                const float m = sample_mask<KIND, false>(atlas, tmpl, g.Ht, g.Wt, tx, ty, nullptr, nullptr);
+              if (inside || !(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
+                float tx, ty;
+                const float m = pair_mask<KIND, false>(g, atlas, toff, g1, dx, dy, &tx, &ty, nullptr, nullptr);
                 if (STATS) ++n_cand;
                 if (m > 1e-6f) {
                   if (STATS) ++n_frag;
@@ -162,7 +183,7 @@ struct TileWalker {
                                            const void* __restrict__ atlas, const int* __restrict__ idx,
                                            float4 (*s_pi)[4], int* s_id, float (*s_part)[kChunk][8],
                                            int* s_kmax, const float (&gC)[NP][3], const float (&gA)[NP],
-                                           const float (&Tl)[NP], const int (&lp)[NP], double* __restrict__ gacc) {
+                                           float (&Ts)[NP], const int (&lp)[NP], double* __restrict__ gacc) {
     int my_max = -1;
 #pragma unroll
     for (int p = 0; p < NP; ++p) my_max = max(my_max, lp[p]);
@@ -174,10 +195,11 @@ struct TileWalker {
     const int kmax = *s_kmax;
     if (kmax < 0) return;
 
-    float Ts[NP], R[NP][3], B[NP];
+    // Ts[p] holds the T entering the last fragment processed; on entry it is
+    // the stored T entering the pixel's last contributor.
+    float R[NP][3], B[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      Ts[p] = Tl[p];
       R[p][0] = R[p][1] = R[p][2] = 0.f;
       B[p] = 1.f;
     }
@@ -192,25 +214,25 @@ struct TileWalker {
         for (int k = 0; k < 8; ++k) acc[k] = 0.f;
         bool any = false;
         const float4 g0 = s_pi[e][0];
-        const int tmpl = __float_as_int(s_pi[e][3].x);
-        if (pos <= warp_max && tmpl >= 0 && !footprint_miss(g0, fx0, fx1, fy0, fy1)) {
+        const int toff = __float_as_int(s_pi[e][3].x);
+        if (pos <= warp_max && toff != kNoFrag && !footprint_miss(g0, fx0, fx1, fy0, fy1)) {
+          const bool inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
           const float4 g1 = s_pi[e][1];
           const float4 g2 = s_pi[e][2];
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
             if (pos <= lp[p]) {
               const float dx = (float)px[p] - g0.x, dy = (float)py[p] - g0.y;
-              if (!(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
-                const float tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
-                const float ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
-                float gx, gy;
-                const float m = sample_mask<KIND, true>(atlas, tmpl, g.Ht, g.Wt, tx, ty, &gx, &gy);
+              if (inside || !(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
+                float tx, ty, gx, gy;
+                const float m = pair_mask<KIND, true>(g, atlas, toff, g1, dx, dy, &tx, &ty, &gx, &gy);
                 if (m > 1e-6f) {
                   const float a = g2.x * m;
                   const float om = fmaxf(1.f - a, 0.f);
                   // T entering this fragment: stored for the last contributor,
-                  // otherwise undo the forward product (om >= t_stop > 0 here).
-                  const float Tk = (pos == lp[p]) ? Tl[p] : __fdiv_rn(Ts[p], om);
+                  // otherwise undo the forward product (om >= t_stop > 0 here,
+                  // so the 2-ulp fast division stays well conditioned).
+                  const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
                   Ts[p] = Tk;
                   const float G = gC[p][0] * (g2.y - R[p][0]) + gC[p][1] * (g2.z - R[p][1]) +
                                   gC[p][2] * (g2.w - R[p][2]) + gA[p] * B[p];
@@ -324,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) count_kernel(Geom g, const PrimInfo*
 }
 
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreads) backward_kernel(Geom g, const PrimInfo* __restrict__ prims,
+__global__ void __launch_bounds__(kThreads, 3) backward_kernel(Geom g, const PrimInfo* __restrict__ prims,
                                                             const void* __restrict__ atlas,
                                                             const int* __restrict__ offs, const int* __restrict__ idx,
                                                             const float* __restrict__ T_last,
@@ -401,7 +423,7 @@ __global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const f
 //   dL/dC = 2 (rendered - target) / (3HW),  dL/dA = -sum_c dL/dC_c * bg_c.
 // loss_out (f64, may be null) receives sum((rendered - target)^2) / (3HW).
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreads) fused_kernel(Geom g, const PrimInfo* __restrict__ prims,
+__global__ void __launch_bounds__(kThreads, 3) fused_kernel(Geom g, const PrimInfo* __restrict__ prims,
                                                          const void* __restrict__ atlas,
                                                          const int* __restrict__ offs, const int* __restrict__ idx,
                                                          const float* __restrict__ target,
@@ -464,6 +486,8 @@ __global__ void __launch_bounds__(kThreads) fused_kernel(Geom g, const PrimInfo*
     case ATLAS_F32_QUAD: { constexpr int KD = ATLAS_F32_QUAD; __VA_ARGS__; } break;   \
     case ATLAS_F16_QUAD: { constexpr int KD = ATLAS_F16_QUAD; __VA_ARGS__; } break;   \
     case ATLAS_BF16_QUAD: { constexpr int KD = ATLAS_BF16_QUAD; __VA_ARGS__; } break; \
+    case ATLAS_F16_PAIR: { constexpr int KD = ATLAS_F16_PAIR; __VA_ARGS__; } break;   \
+    case ATLAS_BF16_PAIR: { constexpr int KD = ATLAS_BF16_PAIR; __VA_ARGS__; } break; \
     default: set_error("unknown atlas kind %d", kind); return DBMP_ERR_INVALID;       \
   }
 

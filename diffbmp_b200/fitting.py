@@ -80,7 +80,8 @@ class ImageFitter:
         self.step_count = torch.zeros(1, dtype=torch.int32, device=dev)
         self.flags = torch.zeros(2, dtype=torch.int32, device=dev)    # [L, overflow]
         self.prim_info = torch.empty((max(self.N, 1), 16), dtype=torch.float32, device=dev)
-        self.offsets = torch.empty(self.rz.T + 1, dtype=torch.int32, device=dev)
+        # zero lists until the first successful binning: an overflowed first bin renders nothing
+        self.offsets = torch.zeros(self.rz.T + 1, dtype=torch.int32, device=dev)
         if not cfg.fused:
             self.color = torch.empty((self.H, self.W, 3), dtype=torch.float32, device=dev)
             self.alpha = torch.empty((self.H, self.W), dtype=torch.float32, device=dev)

@@ -22,12 +22,14 @@ from typing import Optional
 import torch
 
 from . import _lib
-from ._lib import (ATLAS_BF16_QUAD, ATLAS_F16_QUAD, ATLAS_F32, ATLAS_F32_QUAD, BIN_CONTENT, BIN_CULL,
-                   Canvas, DbmpError, call, lib)
+from ._lib import (ATLAS_BF16_PAIR, ATLAS_BF16_QUAD, ATLAS_F16_PAIR, ATLAS_F16_QUAD, ATLAS_F32, ATLAS_F32_QUAD,
+                   BIN_CONTENT, BIN_CULL, Canvas, DbmpError, call, lib)
 
-KIND_NAMES = {"f32": ATLAS_F32, "f32q": ATLAS_F32_QUAD, "f16": ATLAS_F16_QUAD, "bf16": ATLAS_BF16_QUAD}
-_KIND_DTYPE = {ATLAS_F32: torch.float32, ATLAS_F32_QUAD: torch.float32, ATLAS_F16_QUAD: torch.float16,
-               ATLAS_BF16_QUAD: torch.bfloat16}
+# Atlas storage kinds: "f32" is the reference layout; the precision form
+# stores half / bfloat16 texels as horizontal pairs ("f16", "bf16", two 4-byte
+# loads per bilinear sample) or as full bilinear quads ("f16q", "bf16q", "f32q").
+KIND_NAMES = {"f32": ATLAS_F32, "f32q": ATLAS_F32_QUAD, "f16q": ATLAS_F16_QUAD, "bf16q": ATLAS_BF16_QUAD,
+              "f16": ATLAS_F16_PAIR, "bf16": ATLAS_BF16_PAIR}
 
 DEFAULT_T_STOP = 1e-7
 
@@ -66,7 +68,8 @@ class Atlas:
         if self.kind == ATLAS_F32:
             self.data = self.templates
         else:
-            self.data = torch.empty((self.P, self.Ht, self.Wt, 4), dtype=_KIND_DTYPE[self.kind], device=t.device)
+            nbytes = int(lib.dbmp_atlas_bytes(self.P, self.Ht, self.Wt, self.kind))
+            self.data = torch.empty(nbytes, dtype=torch.uint8, device=t.device)
             call("dbmp_atlas_pack", _ptr(self.templates), self.P, self.Ht, self.Wt, self.kind, _ptr(self.data), st)
 
     def with_kind(self, kind) -> "Atlas":

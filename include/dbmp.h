@@ -41,6 +41,8 @@ typedef enum {
 #define DBMP_ATLAS_F32_QUAD 1   /* (P,Ht,Wt,4) f32 bilinear quads, see dbmp_atlas_pack */
 #define DBMP_ATLAS_F16_QUAD 2   /* (P,Ht,Wt,4) IEEE half quads */
 #define DBMP_ATLAS_BF16_QUAD 3  /* (P,Ht,Wt,4) bfloat16 quads */
+#define DBMP_ATLAS_F16_PAIR 4   /* (P,Ht+1,Wt,2) IEEE half horizontal pairs, see dbmp_atlas_pack */
+#define DBMP_ATLAS_BF16_PAIR 5  /* (P,Ht+1,Wt,2) bfloat16 horizontal pairs */
 
 /* Binning modes (dbmp_canvas.bin_mode). */
 #define DBMP_BIN_CONTENT 0  /* world bbox of the template's texels > 1e-6:
@@ -74,11 +76,14 @@ int dbmp_num_tiles(const dbmp_canvas* cv);
 int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* out_bbox,
                          void* stream);
 
-/* Repacks a (P,Ht,Wt) f32 atlas into kind DBMP_ATLAS_{F32,F16,BF16}_QUAD:
- * element (p,y,x) holds the bilinear neighbours t[y][x], t[y][x+1],
- * t[y+1][x], t[y+1][x+1] (0 outside the template).  out holds P*Ht*Wt*4
- * elements of the kind's type.  No reference counterpart (storage format of
- * the precision form). */
+/* Repacks a (P,Ht,Wt) f32 atlas into a storage kind of the precision form:
+ * *_QUAD: element (p,y,x) holds the bilinear neighbours t[y][x], t[y][x+1],
+ *   t[y+1][x], t[y+1][x+1]; out holds P*Ht*Wt*4 elements;
+ * *_PAIR: element (p,y,x) holds t[y][x], t[y][x+1] for y < Ht plus one zero
+ *   row y = Ht; out holds P*(Ht+1)*Wt*2 elements.
+ * Neighbours outside the template are 0.  dbmp_atlas_bytes gives the size.
+ * No reference counterpart (storage format of the precision form). */
+size_t dbmp_atlas_bytes(int P, int Ht, int Wt, int kind);
 int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, void* out, void* stream);
 
 /* Scratch bytes that dbmp_bin needs for `capacity` tile-list entries. */
@@ -87,7 +92,9 @@ size_t dbmp_bin_workspace_bytes(const dbmp_canvas* cv, long long capacity);
 size_t dbmp_prim_info_bytes(int num_prims);
 
 /* Per-primitive preparation only (for callers that supply their own tile
- * lists): fills prim_info (dbmp_prim_info_bytes(N) bytes, 16-byte aligned). */
+ * lists): fills prim_info (dbmp_prim_info_bytes(N) bytes, 16-byte aligned).
+ * prim_info records atlas offsets for cv->atlas_kind: pass it only to calls
+ * made with the same atlas_kind and template shape. */
 int dbmp_prepare(const dbmp_canvas* cv, const float* means2D, const float* radii,
                  const float* rotations, const float* opacities, const float* colors,
                  const int32_t* sel, void* prim_info, void* stream);

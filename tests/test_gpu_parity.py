@@ -154,6 +154,24 @@ def test_backward_parity_gpu(name):
     check_grads(sc, offs, idx, gc, ga, ours)
 
 
+@pytest.mark.parametrize("kind", ["f32q", "f16", "f16q", "bf16", "bf16q"])
+def test_storage_kinds_track_fp32_gpu(kind):
+    """Every storage kind renders within its quantisation error of the FP32
+    kernels and yields gradients within 1e-2 (half) / 5e-2 (bfloat16) relative."""
+    sc = SCENES["atlas128"]()
+    c32, a32, st32, rz, atlas32, d = ours_forward(sc)
+    ck, ak, stk, rzk, atlask, _ = ours_forward(sc, kind=kind)
+    tol = {"f32q": 1e-5, "f16": 2e-3, "f16q": 2e-3, "bf16": 2e-2, "bf16q": 2e-2}[kind]
+    assert np.abs(ck - c32).max() <= tol
+    rng = np.random.default_rng(2)
+    gc = torch.from_numpy(rng.normal(0, 1, (sc.H, sc.W, 3)).astype(np.float32)).cuda()
+    g32 = rz.backward(st32, gc, None, d["radii"], d["rotations"], d["opacities"], d["colors"], atlas32)
+    gk = rzk.backward(stk, gc, None, d["radii"], d["rotations"], d["opacities"], d["colors"], atlask)
+    gtol = {"f32q": 1e-4, "f16": 1e-2, "f16q": 1e-2, "bf16": 5e-2, "bf16q": 5e-2}[kind]
+    for a, b in zip(gk, g32):
+        assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < gtol
+
+
 def test_caller_mapping_equals_device_binning_gpu():
     """A caller-supplied reference mapping and the device binning render the same image."""
     sc = SCENES["atlas128"]()
@@ -179,7 +197,8 @@ def test_autograd_function_gpu():
     check_grads(sc, offs, idx, wc.cpu().numpy(), wa.cpu().numpy(), ours)
 
 
-@pytest.mark.parametrize("kind,min_psnr", [("f32q", 90.0), ("f16", 60.0), ("bf16", 45.0)])
+@pytest.mark.parametrize("kind,min_psnr", [("f32q", 90.0), ("f16", 60.0), ("f16q", 60.0), ("bf16", 45.0),
+                                           ("bf16q", 45.0)])
 def test_precision_forms_gpu(kind, min_psnr):
     sc = SCENES["atlas128"]()
     offs, idx = bin_scene(sc)
