@@ -11,7 +11,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdbmp.so")
+# DBMP_LIBRARY selects another build of the same ABI (e.g. a tuning variant).
+LIB_PATH = os.environ.get("DBMP_LIBRARY") or os.path.join(HERE, "libdbmp.so")
 
 DBMP_OK, DBMP_ERR_INVALID, DBMP_ERR_CUDA, DBMP_ERR_CAPACITY, DBMP_ERR_UNSUPPORTED = range(5)
 ATLAS_F32, ATLAS_F32_QUAD, ATLAS_F16_QUAD, ATLAS_BF16_QUAD, ATLAS_F16_PAIR, ATLAS_BF16_PAIR = range(6)

@@ -205,7 +205,7 @@ int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas, 
   if (rc) return rc;
   REQUIRE(atlas && tile_offsets && tile_indices && counts, "dbmp_count: null pointer");
   REQUIRE(g.N == 0 || prim_info, "dbmp_count: prim_info is null");
-  cudaError_t e = cudaMemsetAsync(counts, 0, 3 * sizeof(unsigned long long), (cudaStream_t)stream);
+  cudaError_t e = cudaMemsetAsync(counts, 0, 6 * sizeof(unsigned long long), (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(counts)");
   return launch_count(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, counts,
                       (cudaStream_t)stream);

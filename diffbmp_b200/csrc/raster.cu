@@ -1,37 +1,39 @@
 // Forward / backward / fused tile compositing kernels.
 //
-// One CTA of 256 threads owns one tile of TS x TS pixels (TS = 32: four
-// pixels per thread, TS = 16: one).  Each warp owns a compact footprint
-// (16x8 or 8x4 pixels) so that a primitive's square cull is mostly warp
-// uniform and the warp's texel fetches stay close together in the atlas.
-// The tile's primitive list is walked in chunks of CH entries whose 64-byte
-// PrimInfo records are staged in shared memory once per CTA; warps that have
-// finished (every pixel below t_stop) skip the math but keep joining the
-// chunk barriers.
+// One CTA owns one tile of TS x TS pixels; each thread owns NP pixels
+// (NP = 4, 2 or 1) of a compact warp footprint (16x8, 16x4 or 8x4 pixels) so
+// that a primitive's square cull is mostly warp-uniform and the warp's texel
+// fetches stay close together in the atlas.  The tile's primitive list is
+// walked in chunks of kChunk entries whose 64-byte PrimInfo records are staged
+// in shared memory once per CTA.  Per entry a thread first computes the texel
+// coordinates of all its pixels and issues all their texel loads (addresses
+// of pixels without a fragment are redirected to texel 0 of the template, so
+// every load is in bounds), then composites them branch-free; warps whose
+// pixels are all below t_stop skip the math but keep joining the barriers.
 #include "dbmp_internal.cuh"
 
 namespace dbmp {
 
-constexpr int kThreads = 256;
 constexpr int kChunk = 32;   // list entries staged per barrier
 
-template <int TS> struct PixLayout;
-template <> struct PixLayout<32> { static constexpr int NP = 4, FW = 16, FH = 8; };
-template <> struct PixLayout<16> { static constexpr int NP = 1, FW = 8, FH = 4; };
-
-// Pixel p of this thread inside its tile.
-template <int TS>
-__device__ __forceinline__ void pixel_of(int warp, int lane, int p, int* x, int* y) {
-  using L = PixLayout<TS>;
-  *x = (warp & 1) * L::FW + (lane & 7) + 8 * (p & 1);
-  *y = (warp >> 1) * L::FH + (lane >> 3) + 4 * (p >> 1);
-}
+template <int TS, int NP>
+struct Layout {
+  static_assert(NP == 1 || NP == 2 || NP == 4, "pixels per thread");
+  static constexpr int FW = NP >= 2 ? 16 : 8;     // warp footprint
+  static constexpr int FH = NP == 4 ? 8 : 4;
+  static constexpr int WPR = TS / FW;              // warps per footprint row
+  static constexpr int NW = (TS / FW) * (TS / FH);
+  static constexpr int NT = NW * 32;
+  static __device__ __forceinline__ int ox(int p) { return 8 * (p & 1); }
+  static __device__ __forceinline__ int oy(int p) { return 4 * (p >> 1); }
+};
 
 // Stages entries [base, base+n) of the tile list: ids and PrimInfo records.
+template <int NT>
 __device__ __forceinline__ void stage_chunk(const PrimInfo* __restrict__ prims, const int* __restrict__ idx,
                                             int N, int base, int n, float4 (*s_pi)[4], int* s_id) {
-  const int e = threadIdx.x >> 2, q = threadIdx.x & 3;
-  if (e < n) {
+  for (int i = threadIdx.x; i < 4 * n; i += NT) {
+    const int e = i >> 2, q = i & 3;
     const int id = __ldg(idx + base + e);
     float4 v;
     if (id >= 0 && id < N) {
@@ -61,28 +63,74 @@ __device__ __forceinline__ bool footprint_inside(const float4& g0, float x0, flo
          (g0.y + g0.w >= y1 + 1.f);
 }
 
-// Mask of one (pixel, primitive) pair; 0 when the pair yields no fragment.
-template <int KIND, bool GRAD>
-__device__ __forceinline__ float pair_mask(const Geom& g, const void* atlas, int toff, const float4& g1,
-                                           float dx, float dy, float* tx, float* ty, float* gx, float* gy) {
-  *tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
-  *ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
-  if (toff == kSolid) {
-    if (GRAD) { *gx = __int_as_float(0x7fc00000); *gy = *gx; }
-    return 1.f;
+// Texel coordinates, sampling position and fetched neighbours of one pixel.
+struct Sample {
+  float tx, ty, wx, wy;
+  bool ok;    // pixel live, inside the cull square and inside [0,W-1]x[0,H-1]
+  Quad q;
+};
+
+// Phase 1 of an entry: texel coordinates of every pixel of the thread (the
+// inverse affine is linear, so pixel p is pixel 0 plus a multiple of a column
+// of A) and whether the pixel can yield a fragment (live, inside the cull
+// square, inside [0,W-1]x[0,H-1]).
+template <int NP, class L>
+__device__ __forceinline__ void entry_coords(const Geom& g, const float4& g0, const float4& g1, bool inside,
+                                             const float (&pxf)[NP], const float (&pyf)[NP],
+                                             const bool (&live)[NP], Sample (&s)[NP]) {
+  const float dx0 = pxf[0] - g0.x, dy0 = pyf[0] - g0.y;
+  const float tx0 = fmaf(g1.x, dx0, fmaf(g1.y, dy0, g.hx));
+  const float ty0 = fmaf(g1.z, dx0, fmaf(g1.w, dy0, g.hy));
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    float tx = tx0, ty = ty0;
+    if (L::ox(p)) { tx = fmaf((float)L::ox(p), g1.x, tx); ty = fmaf((float)L::ox(p), g1.z, ty); }
+    if (L::oy(p)) { tx = fmaf((float)L::oy(p), g1.y, tx); ty = fmaf((float)L::oy(p), g1.w, ty); }
+    bool cull_ok = inside;
+    if (!inside) cull_ok = !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+    const bool in_rng = tx >= 0.f && tx <= g.wm1 && ty >= 0.f && ty <= g.hm1;
+    s[p].ok = live[p] && cull_ok && in_rng;
+    s[p].tx = tx;
+    s[p].ty = ty;
   }
-  return sample_mask<KIND, GRAD>(atlas, toff, g, *tx, *ty, gx, gy);
+}
+
+// Phase 2 for one pixel: sampling position and texel fetch (texel 0 of the
+// template when the pixel cannot yield a fragment, so the load is in bounds).
+template <int KIND>
+__device__ __forceinline__ void entry_fetch(const Geom& g, const void* __restrict__ atlas, int toff, Sample& s) {
+  const float tx = s.ok ? s.tx : 0.f, ty = s.ok ? s.ty : 0.f;
+  float fx, fy;
+  const int x0 = floor_small(tx, &fx);
+  const int y0 = floor_small(ty, &fy);
+  s.wx = tx - fx;
+  s.wy = ty - fy;
+  s.q = AtlasFetch<KIND>::get(atlas, toff, g.Ht, g.Wt, x0, y0);
+}
+
+// Bilinear mask (clamped) and, with GRAD, its texel-space gradient.
+template <bool GRAD>
+__device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
+  const float dt = s.q.v01 - s.q.v00, db = s.q.v11 - s.q.v10;
+  const float top = fmaf(s.wx, dt, s.q.v00);
+  const float bot = fmaf(s.wx, db, s.q.v10);
+  const float m = fmaf(s.wy, bot - top, top);
+  if (GRAD) {
+    *gx = fmaf(s.wy, db - dt, dt);
+    *gy = bot - top;
+  }
+  return fmaxf(0.f, fminf(1.f, m));
 }
 
 // ---------------------------------------------------------------------------
-// Forward walk for one tile.  Leaves per-pixel colour, final T, the T entering
-// the last contributor and the last contributor's list position.
-template <int TS, int KIND>
+template <int TS, int NP, int KIND>
 struct TileWalker {
-  using L = PixLayout<TS>;
-  static constexpr int NP = L::NP;
+  using L = Layout<TS, NP>;
+  static constexpr int NT = L::NT;
+  static constexpr int NW = L::NW;
 
   int warp, lane, start, end;
+  float pxf[NP], pyf[NP];
   int px[NP], py[NP];
   bool valid[NP];
   float fx0, fx1, fy0, fy1;
@@ -93,77 +141,106 @@ struct TileWalker {
     const int tx = tile % g.tilesX, ty = tile / g.tilesX;
     start = __ldg(offs + tile);
     end = __ldg(offs + tile + 1);
+    const int bx = tx * TS + (warp % L::WPR) * L::FW + (lane & 7);
+    const int by = ty * TS + (warp / L::WPR) * L::FH + (lane >> 3);
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      int x, y;
-      pixel_of<TS>(warp, lane, p, &x, &y);
-      px[p] = tx * TS + x;
-      py[p] = ty * TS + y;
+      px[p] = bx + L::ox(p);
+      py[p] = by + L::oy(p);
+      pxf[p] = (float)px[p];
+      pyf[p] = (float)py[p];
       valid[p] = px[p] < g.W && py[p] < g.H;
     }
-    fx0 = (float)(tx * TS + (warp & 1) * L::FW);
+    fx0 = (float)(tx * TS + (warp % L::WPR) * L::FW);
     fx1 = fx0 + (float)(L::FW - 1);
-    fy0 = (float)(ty * TS + (warp >> 1) * L::FH);
+    fy0 = (float)(ty * TS + (warp / L::WPR) * L::FH);
     fy1 = fy0 + (float)(L::FH - 1);
   }
 
-  // STATS: count (pixel, primitive) pairs that pass the cull and fragments
-  // composited, both before termination, into cnt[0], cnt[1].
+  // Forward walk.  STATS: counts (pixel, primitive) pairs that pass the cull
+  // and fragments composited, both before termination, plus walk statistics.
   template <bool STATS = false>
   __device__ __forceinline__ void forward(const Geom& g, const PrimInfo* __restrict__ prims,
                                           const void* __restrict__ atlas, const int* __restrict__ idx,
                                           float4 (*s_pi)[4], int* s_id,
                                           float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP],
                                           unsigned long long* cnt = nullptr) {
-    unsigned long long n_cand = 0, n_frag = 0;
-    bool done[NP];
+    unsigned long long n_cand = 0, n_frag = 0, n_went = 0, n_slots = 0, n_miss = 0;
+    bool live[NP];
     bool all_done = true;
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
       C[p][0] = C[p][1] = C[p][2] = 0.f;
       T[p] = 1.f; Tl[p] = 1.f; lp[p] = -1;
-      done[p] = !valid[p];
-      all_done = all_done && done[p];
+      live[p] = valid[p];
+      all_done = all_done && !live[p];
     }
     bool warp_done = __all_sync(0xffffffffu, all_done);
     for (int base = start; base < end; base += kChunk) {
       const int n = min(kChunk, end - base);
-      stage_chunk(prims, idx, g.N, base, n, s_pi, s_id);
+      stage_chunk<NT>(prims, idx, g.N, base, n, s_pi, s_id);
       __syncthreads();
       if (!warp_done) {
         for (int e = 0; e < n; ++e) {
           const float4 g0 = s_pi[e][0];
-          if (footprint_miss(g0, fx0, fx1, fy0, fy1)) continue;
+          if (footprint_miss(g0, fx0, fx1, fy0, fy1)) {
+            if (STATS) ++n_miss;
+            continue;
+          }
           const int toff = __float_as_int(s_pi[e][3].x);
           if (toff == kNoFrag) continue;
-          const bool inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
           const float4 g1 = s_pi[e][1];
           const float4 g2 = s_pi[e][2];
           const int pos = base - start + e;
+          if (STATS) {
+            ++n_went;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) n_slots += __popc(__ballot_sync(0xffffffffu, live[p]));
+          }
+          Sample s[NP];
+          float m[NP];
+          if (toff != kSolid) {
+            entry_coords<NP, L>(g, g0, g1, footprint_inside(g0, fx0, fx1, fy0, fy1), pxf, pyf, live, s);
+            bool any[NP];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              any[p] = __any_sync(0xffffffffu, s[p].ok);
+              if (any[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
+            }
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              m[p] = any[p] ? blend<false>(s[p], nullptr, nullptr) : 0.f;
+              if (STATS) {
+                const bool c = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+                n_cand += c;
+              }
+            }
+          } else {
+            // NaN geometry: every live pixel that passes the cull gets mask 1
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              s[p].ok = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+              m[p] = 1.f;
+              if (STATS) n_cand += s[p].ok;
+            }
+          }
           bool local_done = true;
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
-            if (!done[p]) {
-              const float dx = (float)px[p] - g0.x, dy = (float)py[p] - g0.y;
-              if (inside || !(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
-                float tx, ty;
-                const float m = pair_mask<KIND, false>(g, atlas, toff, g1, dx, dy, &tx, &ty, nullptr, nullptr);
-                if (STATS) ++n_cand;
-                if (m > 1e-6f) {
-                  if (STATS) ++n_frag;
-                  const float a = g2.x * m;
-                  const float w = T[p] * a;
-                  C[p][0] = fmaf(w, g2.y, C[p][0]);
-                  C[p][1] = fmaf(w, g2.z, C[p][1]);
-                  C[p][2] = fmaf(w, g2.w, C[p][2]);
-                  Tl[p] = T[p];
-                  lp[p] = pos;
-                  T[p] *= fmaxf(1.f - a, 0.f);
-                  if (T[p] < g.t_stop) done[p] = true;
-                }
-              }
+            const bool frag = s[p].ok && m[p] > 1e-6f;
+            if (STATS) n_frag += frag;
+            if (__any_sync(0xffffffffu, frag)) {
+              const float a = frag ? g2.x * m[p] : 0.f;
+              const float w = T[p] * a;
+              C[p][0] = fmaf(w, g2.y, C[p][0]);
+              C[p][1] = fmaf(w, g2.z, C[p][1]);
+              C[p][2] = fmaf(w, g2.w, C[p][2]);
+              Tl[p] = frag ? T[p] : Tl[p];
+              lp[p] = frag ? pos : lp[p];
+              T[p] *= fmaxf(1.f - a, 0.f);
+              live[p] = live[p] && !(T[p] < g.t_stop);
             }
-            local_done = local_done && done[p];
+            local_done = local_done && !live[p];
           }
           if (__all_sync(0xffffffffu, local_done)) { warp_done = true; break; }
         }
@@ -173,12 +250,18 @@ struct TileWalker {
     if (STATS) {
       atomicAdd(cnt + 0, n_cand);
       atomicAdd(cnt + 1, n_frag);
+      if (lane == 0) {
+        atomicAdd(cnt + 3, n_went);
+        atomicAdd(cnt + 4, n_slots);
+        atomicAdd(cnt + 5, n_miss);
+      }
     }
   }
 
-  // Reverse walk.  gC/gA are the upstream gradients of each pixel.  Partial
-  // per-primitive sums are reduced in the warp, then across the CTA, and
-  // accumulated into gacc (N,8) f64.
+  // Reverse walk.  gC/gA: upstream gradients per pixel; Ts: on entry the T
+  // entering each pixel's last contributor (lp).  Per-primitive partial sums
+  // are reduced in the warp, then across the CTA, and accumulated into gacc
+  // (N,8) f64 (layout documented at finalize_kernel).
   __device__ __forceinline__ void backward(const Geom& g, const PrimInfo* __restrict__ prims,
                                            const void* __restrict__ atlas, const int* __restrict__ idx,
                                            float4 (*s_pi)[4], int* s_id, float (*s_part)[kChunk][8],
@@ -195,17 +278,18 @@ struct TileWalker {
     const int kmax = *s_kmax;
     if (kmax < 0) return;
 
-    // Ts[p] holds the T entering the last fragment processed; on entry it is
-    // the stored T entering the pixel's last contributor.
-    float R[NP][3], B[NP];
+    // H = gC . R and B = prod(1 - a) over the fragments behind the current
+    // one, where R is their colour composited from T = 1; both obey
+    // X_{k-1} = (1 - a_k) X_k + a_k x_k, so dL/da_k = T_k (gC.c_k - H + gA B).
+    float H[NP], B[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      R[p][0] = R[p][1] = R[p][2] = 0.f;
+      H[p] = 0.f;
       B[p] = 1.f;
     }
     for (int cb = (kmax / kChunk) * kChunk; cb >= 0; cb -= kChunk) {
       const int n = min(kChunk, end - start - cb);
-      stage_chunk(prims, idx, g.N, start + cb, n, s_pi, s_id);
+      stage_chunk<NT>(prims, idx, g.N, start + cb, n, s_pi, s_id);
       __syncthreads();
       for (int e = n - 1; e >= 0; --e) {
         const int pos = cb + e;
@@ -216,45 +300,65 @@ struct TileWalker {
         const float4 g0 = s_pi[e][0];
         const int toff = __float_as_int(s_pi[e][3].x);
         if (pos <= warp_max && toff != kNoFrag && !footprint_miss(g0, fx0, fx1, fy0, fy1)) {
-          const bool inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
           const float4 g1 = s_pi[e][1];
           const float4 g2 = s_pi[e][2];
+          bool live[NP];
+#pragma unroll
+          for (int p = 0; p < NP; ++p) live[p] = pos <= lp[p];
+          Sample s[NP];
+          float m[NP], gx[NP], gy[NP];
+          bool anyp[NP];
+          if (toff != kSolid) {
+            entry_coords<NP, L>(g, g0, g1, footprint_inside(g0, fx0, fx1, fy0, fy1), pxf, pyf, live, s);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              anyp[p] = __any_sync(0xffffffffu, s[p].ok);
+              if (anyp[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
+            }
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              m[p] = 0.f; gx[p] = gy[p] = 0.f;
+              if (anyp[p]) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
+            }
+          } else {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              const float dx = pxf[p] - g0.x, dy = pyf[p] - g0.y;
+              s[p].ok = live[p] && !(fabsf(dx) > g0.z || fabsf(dy) > g0.w);
+              s[p].tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
+              s[p].ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
+              m[p] = 1.f;
+              gx[p] = gy[p] = __int_as_float(0x7fc00000);
+            }
+          }
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
-            if (pos <= lp[p]) {
-              const float dx = (float)px[p] - g0.x, dy = (float)py[p] - g0.y;
-              if (inside || !(fabsf(dx) > g0.z || fabsf(dy) > g0.w)) {
-                float tx, ty, gx, gy;
-                const float m = pair_mask<KIND, true>(g, atlas, toff, g1, dx, dy, &tx, &ty, &gx, &gy);
-                if (m > 1e-6f) {
-                  const float a = g2.x * m;
-                  const float om = fmaxf(1.f - a, 0.f);
-                  // T entering this fragment: stored for the last contributor,
-                  // otherwise undo the forward product (om >= t_stop > 0 here,
-                  // so the 2-ulp fast division stays well conditioned).
-                  const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
-                  Ts[p] = Tk;
-                  const float G = gC[p][0] * (g2.y - R[p][0]) + gC[p][1] * (g2.z - R[p][1]) +
-                                  gC[p][2] * (g2.w - R[p][2]) + gA[p] * B[p];
-                  const float dLda = Tk * G;
-                  const float ex = tx - g.hx, ey = ty - g.hy;
-                  acc[0] = fmaf(dLda, gx, acc[0]);
-                  acc[1] = fmaf(dLda, gy, acc[1]);
-                  acc[2] = fmaf(dLda, fmaf(gx, ex, gy * ey), acc[2]);
-                  acc[3] = fmaf(dLda, fmaf(gx * ey, g.rxy, -gy * ex * g.ryx), acc[3]);
-                  const float w = a * Tk;
-                  acc[4] = fmaf(gC[p][0], w, acc[4]);
-                  acc[5] = fmaf(gC[p][1], w, acc[5]);
-                  acc[6] = fmaf(gC[p][2], w, acc[6]);
-                  acc[7] = fmaf(dLda, a, acc[7]);
-                  R[p][0] = fmaf(om, R[p][0], g2.y * a);
-                  R[p][1] = fmaf(om, R[p][1], g2.z * a);
-                  R[p][2] = fmaf(om, R[p][2], g2.w * a);
-                  B[p] *= om;
-                  any = true;
-                }
-              }
-            }
+            const bool frag = s[p].ok && m[p] > 1e-6f;
+            if (!__any_sync(0xffffffffu, frag)) continue;
+            const float a = frag ? g2.x * m[p] : 0.f;
+            const float om = fmaxf(1.f - a, 0.f);
+            // T entering this fragment: stored for the last contributor, else
+            // undo the forward product (om >= t_stop > 0 for every earlier
+            // fragment, so the fast division is well conditioned; om = 1 and
+            // Ts is unchanged when there is no fragment).
+            const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
+            Ts[p] = Tk;
+            const float gCc = fmaf(gC[p][0], g2.y, fmaf(gC[p][1], g2.z, gC[p][2] * g2.w));
+            const float dLda = frag ? Tk * (gCc - H[p] + gA[p] * B[p]) : 0.f;
+            const float u = dLda * gx[p], v = dLda * gy[p];
+            const float ex = s[p].tx - g.hx, ey = s[p].ty - g.hy;
+            acc[0] += u;
+            acc[1] += v;
+            acc[2] = fmaf(u, ex, fmaf(v, ey, acc[2]));
+            acc[3] = fmaf(u * g.rxy, ey, fmaf(-v * g.ryx, ex, acc[3]));
+            const float w = a * Tk;
+            acc[4] = fmaf(gC[p][0], w, acc[4]);
+            acc[5] = fmaf(gC[p][1], w, acc[5]);
+            acc[6] = fmaf(gC[p][2], w, acc[6]);
+            acc[7] = fmaf(dLda, a, acc[7]);
+            H[p] = fmaf(om, H[p], a * gCc);
+            B[p] *= om;
+            any = any || frag;
           }
         }
         if (__any_sync(0xffffffffu, any)) {
@@ -286,12 +390,12 @@ struct TileWalker {
         }
       }
       __syncthreads();
-      // CTA reduction over the 8 warps; one f64 atomic per non-zero sum.
-      for (int i = threadIdx.x; i < n * 8; i += kThreads) {
+      // CTA reduction over the warps; one f64 atomic per non-zero sum.
+      for (int i = threadIdx.x; i < n * 8; i += NT) {
         const int e = i >> 3, k = i & 7;
         float s = 0.f;
 #pragma unroll
-        for (int w = 0; w < kThreads / 32; ++w) s += s_part[w][e][k];
+        for (int w = 0; w < NW; ++w) s += s_part[w][e][k];
         if (s != 0.f && s_id[e] >= 0) atomicAdd(gacc + (size_t)s_id[e] * 8 + k, (double)s);
       }
       __syncthreads();
@@ -299,18 +403,32 @@ struct TileWalker {
   }
 };
 
+// Pixels per thread of each tile size (tuned on B200).
+template <int TS> struct DefaultNP;
+#ifndef DBMP_NP32
+#define DBMP_NP32 2
+#endif
+template <> struct DefaultNP<32> { static constexpr int v = DBMP_NP32; };
+template <> struct DefaultNP<16> { static constexpr int v = 1; };
+
+template <int TS> constexpr int kThreadsOf() { return Layout<TS, DefaultNP<TS>::v>::NT; }
+// Resident CTAs per SM the register allocation is bounded for (walk kernels).
+#ifndef DBMP_MINBLOCKS256
+#define DBMP_MINBLOCKS256 3
+#endif
+template <int TS> constexpr int kBlocksPerSM() { return kThreadsOf<TS>() >= 512 ? 2 : DBMP_MINBLOCKS256; }
+
 // ---------------------------------------------------------------------------
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreads) forward_kernel(Geom g, const PrimInfo* __restrict__ prims,
-                                                           const void* __restrict__ atlas,
-                                                           const int* __restrict__ offs, const int* __restrict__ idx,
-                                                           float* __restrict__ out_color, float* __restrict__ out_alpha,
-                                                           float* __restrict__ T_last, int* __restrict__ last_pos) {
+__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) forward_kernel(
+    Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
+    const int* __restrict__ idx, float* __restrict__ out_color, float* __restrict__ out_alpha,
+    float* __restrict__ T_last, int* __restrict__ last_pos) {
+  constexpr int NP = DefaultNP<TS>::v;
   __shared__ float4 s_pi[kChunk][4];
   __shared__ int s_id[kChunk];
-  TileWalker<TS, KIND> tw;
+  TileWalker<TS, NP, KIND> tw;
   tw.init(g, blockIdx.x, offs);
-  constexpr int NP = TileWalker<TS, KIND>::NP;
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
   tw.forward(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp);
@@ -330,15 +448,16 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(Geom g, const PrimInf
 // Counting pass (diagnostics / roofline accounting): same walk as the
 // forward, no outputs except the counters.
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreads) count_kernel(Geom g, const PrimInfo* __restrict__ prims,
-                                                         const void* __restrict__ atlas,
-                                                         const int* __restrict__ offs, const int* __restrict__ idx,
-                                                         unsigned long long* __restrict__ cnt) {
+__global__ void __launch_bounds__(kThreadsOf<TS>()) count_kernel(Geom g, const PrimInfo* __restrict__ prims,
+                                                                 const void* __restrict__ atlas,
+                                                                 const int* __restrict__ offs,
+                                                                 const int* __restrict__ idx,
+                                                                 unsigned long long* __restrict__ cnt) {
+  constexpr int NP = DefaultNP<TS>::v;
   __shared__ float4 s_pi[kChunk][4];
   __shared__ int s_id[kChunk];
-  TileWalker<TS, KIND> tw;
+  TileWalker<TS, NP, KIND> tw;
   tw.init(g, blockIdx.x, offs);
-  constexpr int NP = TileWalker<TS, KIND>::NP;
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
   tw.template forward<true>(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp, cnt);
@@ -346,22 +465,19 @@ __global__ void __launch_bounds__(kThreads) count_kernel(Geom g, const PrimInfo*
 }
 
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreads, 3) backward_kernel(Geom g, const PrimInfo* __restrict__ prims,
-                                                            const void* __restrict__ atlas,
-                                                            const int* __restrict__ offs, const int* __restrict__ idx,
-                                                            const float* __restrict__ T_last,
-                                                            const int* __restrict__ last_pos,
-                                                            const float* __restrict__ grad_color,
-                                                            const float* __restrict__ grad_alpha,
-                                                            double* __restrict__ gacc) {
+__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward_kernel(
+    Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
+    const int* __restrict__ idx, const float* __restrict__ T_last, const int* __restrict__ last_pos,
+    const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc) {
+  constexpr int NP = DefaultNP<TS>::v;
+  using TW = TileWalker<TS, NP, KIND>;
   __shared__ float4 s_pi[kChunk][4];
   __shared__ int s_id[kChunk];
-  __shared__ float s_part[kThreads / 32][kChunk][8];
+  __shared__ float s_part[TW::NW][kChunk][8];
   __shared__ int s_kmax;
-  TileWalker<TS, KIND> tw;
+  TW tw;
   tw.init(g, blockIdx.x, offs);
-  constexpr int NP = TileWalker<TS, KIND>::NP;
-  float gC[NP][3], gA[NP], Tl[NP];
+  float gC[NP][3], gA[NP], Ts[NP];
   int lp[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
@@ -371,14 +487,14 @@ __global__ void __launch_bounds__(kThreads, 3) backward_kernel(Geom g, const Pri
       gC[p][1] = grad_color[3 * q + 1];
       gC[p][2] = grad_color[3 * q + 2];
       gA[p] = grad_alpha ? grad_alpha[q] : 0.f;
-      Tl[p] = T_last[q];
+      Ts[p] = T_last[q];
       lp[p] = last_pos[q];
     } else {
       gC[p][0] = gC[p][1] = gC[p][2] = 0.f;
-      gA[p] = 0.f; Tl[p] = 1.f; lp[p] = -1;
+      gA[p] = 0.f; Ts[p] = 1.f; lp[p] = -1;
     }
   }
-  tw.backward(g, prims, atlas, idx, s_pi, s_id, s_part, &s_kmax, gC, gA, Tl, lp, gacc);
+  tw.backward(g, prims, atlas, idx, s_pi, s_id, s_part, &s_kmax, gC, gA, Ts, lp, gacc);
 }
 
 __device__ __forceinline__ double sigmoid_d(double x) {
@@ -389,6 +505,10 @@ __device__ __forceinline__ double sigmoid_d(double x) {
 
 // Converts the accumulated per-primitive sums into the reference's gradient
 // outputs (tile_backward.cu:255-343 chain rule, applied once per primitive).
+// gacc[n] = { S dLda*gx, S dLda*gy, S dLda*(gx*ex + gy*ey),
+//             S dLda*(gx*ey*hx/hy - gy*ex*hy/hx), S gC_r*a*T, S gC_g*a*T,
+//             S gC_b*a*T, S dLda*a }  summed over the primitive's fragments,
+// with (ex, ey) the texel coordinate minus (hx, hy) and gx, gy = d mask/d tex.
 __global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const float* __restrict__ rot,
                                 const float* __restrict__ opac, const float* __restrict__ colors,
                                 const double* __restrict__ gacc, float* __restrict__ g_means,
@@ -423,23 +543,21 @@ __global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const f
 //   dL/dC = 2 (rendered - target) / (3HW),  dL/dA = -sum_c dL/dC_c * bg_c.
 // loss_out (f64, may be null) receives sum((rendered - target)^2) / (3HW).
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreads, 3) fused_kernel(Geom g, const PrimInfo* __restrict__ prims,
-                                                         const void* __restrict__ atlas,
-                                                         const int* __restrict__ offs, const int* __restrict__ idx,
-                                                         const float* __restrict__ target,
-                                                         const float* __restrict__ background,
-                                                         float* __restrict__ out_image, double* __restrict__ gacc,
-                                                         double* __restrict__ loss_out,
-                                                         const int* __restrict__ skip_flag) {
+__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_kernel(
+    Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
+    const int* __restrict__ idx, const float* __restrict__ target, const float* __restrict__ background,
+    float* __restrict__ out_image, double* __restrict__ gacc, double* __restrict__ loss_out,
+    const int* __restrict__ skip_flag) {
   if (skip_flag != nullptr && *skip_flag != 0) return;   // binning overflowed: leave all state untouched
+  constexpr int NP = DefaultNP<TS>::v;
+  using TW = TileWalker<TS, NP, KIND>;
   __shared__ float4 s_pi[kChunk][4];
   __shared__ int s_id[kChunk];
-  __shared__ float s_part[kThreads / 32][kChunk][8];
+  __shared__ float s_part[TW::NW][kChunk][8];
   __shared__ int s_kmax;
-  __shared__ float s_loss[kThreads / 32];
-  TileWalker<TS, KIND> tw;
+  __shared__ float s_loss[TW::NW];
+  TW tw;
   tw.init(g, blockIdx.x, offs);
-  constexpr int NP = TileWalker<TS, KIND>::NP;
   float C[NP][3], T[NP], Tl[NP], gC[NP][3], gA[NP];
   int lp[NP];
   tw.forward(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp);
@@ -472,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, 3) fused_kernel(Geom g, const PrimIn
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) t += s_loss[w];
+      for (int w = 0; w < TW::NW; ++w) t += s_loss[w];
       atomicAdd(loss_out, t * (double)inv);
     }
   }
@@ -480,8 +598,8 @@ __global__ void __launch_bounds__(kThreads, 3) fused_kernel(Geom g, const PrimIn
 }
 
 // ---------------------------------------------------------------------------
-#define DBMP_KIND_SWITCH(kind, ...)                                  \
-  switch (kind) {                                                    \
+#define DBMP_KIND_SWITCH(kind, ...)                                                   \
+  switch (kind) {                                                                     \
     case ATLAS_F32: { constexpr int KD = ATLAS_F32; __VA_ARGS__; } break;             \
     case ATLAS_F32_QUAD: { constexpr int KD = ATLAS_F32_QUAD; __VA_ARGS__; } break;   \
     case ATLAS_F16_QUAD: { constexpr int KD = ATLAS_F16_QUAD; __VA_ARGS__; } break;   \
@@ -499,7 +617,7 @@ __global__ void __launch_bounds__(kThreads, 3) fused_kernel(Geom g, const PrimIn
 int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                    const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, color, alpha, T_last, last_pos))));
   DBMP_CHECK_LAUNCH("forward_kernel");
   return DBMP_OK;
@@ -508,7 +626,7 @@ int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* a
 int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  unsigned long long* cnt, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (count_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (count_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, cnt))));
   DBMP_CHECK_LAUNCH("count_kernel");
   return DBMP_OK;
@@ -518,7 +636,7 @@ int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* 
                     const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
                     const float* grad_alpha, double* gacc, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
                                                    grad_alpha, gacc))));
   DBMP_CHECK_LAUNCH("backward_kernel");
@@ -537,7 +655,7 @@ int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atl
                  const float* target, const float* background, float* out_image, double* gacc, double* loss,
                  const int* skip_flag, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (fused_kernel<TSV, KD><<<g.T, kThreads, 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (fused_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, target, background, out_image,
                                                    gacc, loss, skip_flag))));
   DBMP_CHECK_LAUNCH("fused_kernel");

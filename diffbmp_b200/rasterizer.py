@@ -31,7 +31,7 @@ from ._lib import (ATLAS_BF16_PAIR, ATLAS_BF16_QUAD, ATLAS_F16_PAIR, ATLAS_F16_Q
 KIND_NAMES = {"f32": ATLAS_F32, "f32q": ATLAS_F32_QUAD, "f16q": ATLAS_F16_QUAD, "bf16q": ATLAS_BF16_QUAD,
               "f16": ATLAS_F16_PAIR, "bf16": ATLAS_BF16_PAIR}
 
-DEFAULT_T_STOP = 1e-7
+DEFAULT_T_STOP = 1e-6   # image error <= t_stop * max colour, well inside the 1e-5 parity bar
 
 
 def _ptr(t: Optional[torch.Tensor]):

@@ -153,8 +153,11 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
 /* Counting pass over the same walk as dbmp_forward (no image output):
  * counts[0] = (pixel, primitive) pairs that pass the square cull before the
  * pixel terminates, counts[1] = fragments composited, counts[2] = tile-list
- * entries (sum over tiles).  counts: 3 device u64, zeroed by the call.  Used
- * for roofline accounting; no reference counterpart. */
+ * entries (sum over tiles), counts[3] = (warp, entry) pairs a warp evaluated,
+ * counts[4] = pixel slots still running summed over those pairs, counts[5] =
+ * (warp, entry) pairs rejected by the warp-footprint test.  counts: 6 device
+ * u64, zeroed by the call.  Used for roofline accounting and load analysis;
+ * no reference counterpart. */
 int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
                const int32_t* tile_offsets, const int32_t* tile_indices,
                unsigned long long* counts, void* stream);
