@@ -53,6 +53,8 @@ SIGNATURES = {
     "dbmp_forward": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_backward": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                            _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_backward_noalloc": (_i, [_CP] + [_vp] * 18),
+    "dbmp_backward_noalloc_max_prims": (_i, []),
     "dbmp_count": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_fused_fwd_bwd": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_adam_step": (_i, [_CP, ctypes.c_void_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -150,6 +150,28 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
                   float* grad_means2D, float* grad_radii, float* grad_rotations,
                   float* grad_opacities, float* grad_colors, void* stream);
 
+/* dbmp_backward for callers that cannot allocate device memory (for example
+ * a plug-in whose host owns the device allocator, or a frame loop that must
+ * not allocate once running).  Same inputs, outputs and results as
+ * dbmp_backward, but the (N,8) f64 gradient-sum scratch is a fixed array
+ * inside this library's device module, so there is no grad_accum argument.
+ * Limit: N <= dbmp_backward_noalloc_max_prims() (65536); larger N returns
+ * DBMP_ERR_CAPACITY.  The array takes 4 MiB on every GPU that loads the
+ * library, until exit.  The first call on a device looks up the array's
+ * device address with that device current: make it before any stream
+ * capture.  All calls share the array (zeroed by each call), so calls that
+ * overlap on the GPU race; serialise them.  No counterpart in the reference. */
+int dbmp_backward_noalloc(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+                          const int32_t* tile_offsets, const int32_t* tile_indices,
+                          const float* T_last, const int32_t* last_pos,
+                          const float* grad_color, const float* grad_alpha,
+                          const float* radii, const float* rotations, const float* opacities,
+                          const float* colors, float* grad_means2D, float* grad_radii,
+                          float* grad_rotations, float* grad_opacities, float* grad_colors,
+                          void* stream);
+/* Largest N dbmp_backward_noalloc accepts. */
+int dbmp_backward_noalloc_max_prims(void);
+
 /* Counting pass over the same walk as dbmp_forward (no image output):
  * counts[0] = (pixel, primitive) pairs that pass the square cull before the
  * pixel terminates, counts[1] = fragments composited, counts[2] = tile-list
