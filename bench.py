@@ -36,6 +36,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd iters/s at 2048^2 N=20k (FP16-storage fused vs plain FP32)"
+# DRAM bytes of one fused_kernel launch on the 2048^2 / N=20k scene, from one
+# ncu capture (read 106.9 MB + write 4.7 MB); null for other configs.
+FUSED_DRAM_BYTES_C2 = 111.586e6
 
 
 def parse():
@@ -352,6 +355,7 @@ def main():
     fp32_peak = fp32_simt_peak_tflops(torch)
     achieved = flop / t_kernel / 1e12
 
+    FUSED_DRAM_BYTES = FUSED_DRAM_BYTES_C2 if args.config == "c2" else None
     ms_step = t_fused / args.steps * 1e3
     value = world * args.steps / t_fused
     line = {
@@ -360,7 +364,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.config}: {spec.H}x{spec.W} canvas, N={spec.N}, "
                                f"{spec.templates.shape[0]}x{spec.templates.shape[1]}x{spec.templates.shape[2]} atlas; "
-                               "one fit iteration per step (device binning, fused fwd+L2+bwd, Adam) with FP16-quad atlas "
+                               "one fit iteration per step (device binning, fused fwd+L2+bwd, Adam) with FP16-pair atlas "
                                "storage and FP32 arithmetic, CUDA-graph replay",
                    "canvas": [spec.H, spec.W], "N": spec.N, "tile_size": 32, "t_stop": job.cfg.t_stop,
                    "l2": "per-step working set (target 50 MB + tile lists/sort buffers) exceeds the 126 MB L2",
@@ -371,8 +375,10 @@ def main():
         "speedup_vs_plain_fp32": (world * args.steps / t_fused) / (world * args.steps / t_plain),
         "loss_after": loss_fused,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak, "traffic": None,
-                     "kernel": "fused_kernel<32, F16_QUAD>", "kernel_ms": t_kernel * 1e3,
+                     "frac": achieved / fp32_peak, "traffic": FUSED_DRAM_BYTES,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
+                                       "kernel on this workload (profiles/fused_kernel_c2_f16pair.md)",
+                     "kernel": "fused_kernel<32, F16_PAIR>", "kernel_ms": t_kernel * 1e3,
                      "flop_model": "12*C + 144*F_live (C pairs passing cull, F_live fragments composited)",
                      "C": cand, "F_live": frag, "warp_entries": went, "live_pixel_slots": slots,
                      "footprint_rejects": miss,
