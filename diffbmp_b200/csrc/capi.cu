@@ -54,6 +54,16 @@ int launch_adam(const Geom& g, const AdamArgs& a, const double* gacc, float* mea
                 float* opac, float* colors, float* m1, float* m2, int* step_count, const int* skip_flag,
                 cudaStream_t st);
 
+int launch_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale, int* bbox,
+                      int* sizes, cudaStream_t st);
+int launch_psd_layout(const int* sizes, int N, long long* layer_offsets, long long* blk, long long* total,
+                      cudaStream_t st);
+int launch_psd_layers(int N, int P, int Ht, int Wt, float scale, float alpha_max, float c_blend,
+                      const float* means2D, const float* radii, const float* rot, const float* colors,
+                      const float* vis, const float* tmpl, const int* sel, const int* bbox,
+                      const long long* layer_offsets, const long long* blk, const float* colors_orig, uint8_t* out,
+                      cudaStream_t st);
+
 // Validates a canvas description and derives the launch geometry.
 int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
   if (!cv) { set_error("%s: canvas is null", who); return DBMP_ERR_INVALID; }
@@ -245,6 +255,37 @@ int dbmp_adam_step(const dbmp_canvas* cv, const dbmp_adam_cfg* cfg, const double
   a.clamp = cfg->clamp;
   return launch_adam(g, a, grad_accum, means2D, radii, rotations, opacities, colors, adam_m, adam_v, step_count,
                      skip_flag, (cudaStream_t)stream);
+}
+
+int dbmp_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale, int32_t* out_bbox,
+                    int32_t* out_sizes, void* stream) {
+  REQUIRE(N >= 0 && H > 0 && W > 0, "dbmp_psd_bboxes: bad sizes N=%d H=%d W=%d", N, H, W);
+  REQUIRE(N == 0 || (means2D && radii && out_bbox && out_sizes), "dbmp_psd_bboxes: null pointer");
+  REQUIRE(((uintptr_t)out_bbox & 15) == 0, "dbmp_psd_bboxes: out_bbox must be 16-byte aligned");
+  return launch_psd_bboxes(means2D, radii, N, H, W, scale, out_bbox, out_sizes, (cudaStream_t)stream);
+}
+
+int dbmp_psd_layout(const int32_t* sizes, int N, int64_t* layer_offsets, int64_t* block_offsets,
+                    int64_t* total_bytes, void* stream) {
+  REQUIRE(N >= 0, "dbmp_psd_layout: N=%d", N);
+  REQUIRE(block_offsets && total_bytes && (N == 0 || (sizes && layer_offsets)), "dbmp_psd_layout: null pointer");
+  return launch_psd_layout(sizes, N, (long long*)layer_offsets, (long long*)block_offsets, (long long*)total_bytes,
+                           (cudaStream_t)stream);
+}
+
+int dbmp_psd_layers(const float* means2D, const float* radii, const float* rotations, const float* colors,
+                    const float* visibility, const float* templates, int P, int Ht, int Wt, const int32_t* sel,
+                    const int32_t* bbox, const int64_t* layer_offsets, const int64_t* block_offsets, int N,
+                    float scale, float alpha_max, float c_blend, const float* colors_orig, uint8_t* out,
+                    void* stream) {
+  REQUIRE(N >= 0 && P > 0 && Ht >= 2 && Wt >= 2, "dbmp_psd_layers: bad sizes N=%d P=%d Ht=%d Wt=%d", N, P, Ht, Wt);
+  REQUIRE(N == 0 || (means2D && radii && rotations && colors && visibility && templates && sel && bbox &&
+                     layer_offsets && block_offsets && out), "dbmp_psd_layers: null pointer");
+  REQUIRE(((uintptr_t)bbox & 15) == 0 && ((uintptr_t)out & 3) == 0,
+          "dbmp_psd_layers: bbox must be 16-byte and out 4-byte aligned");
+  return launch_psd_layers(N, P, Ht, Wt, scale, alpha_max, c_blend, means2D, radii, rotations, colors, visibility,
+                           templates, sel, bbox, (const long long*)layer_offsets, (const long long*)block_offsets,
+                           colors_orig, out, (cudaStream_t)stream);
 }
 
 }  // extern "C"

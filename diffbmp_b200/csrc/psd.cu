@@ -1,0 +1,235 @@
+// PSD layer export: one cropped uint8 RGBA layer per primitive.
+//
+// Replaces cuda_tile_rasterizer/cuda_kernels/psd_export_kernels.cu.  The
+// reference launches N x (all 16x16 canvas tiles) blocks and has each thread
+// loop over a canvas tile for its primitive, O(N*H*W) work for O(sum of crop
+// areas) output.  Here a layout pass prefix-sums each layer's byte size and
+// 16x16 block count on the device, and a persistent grid walks only the
+// blocks of the crops, one pixel per thread, writing one uchar4 per pixel.
+//
+// The per-pixel arithmetic must give the reference's bytes exactly, and the
+// reference builds it with --use_fast_math (setup_psd_export.py:69), so this
+// file is compiled with --use_fast_math too and keeps each expression in the
+// reference's operation order (psd_export_common.h:55-121,
+// psd_export_kernels.cu:26-55,96-195).
+#include <cstdint>
+
+#include "dbmp_internal.cuh"
+
+namespace dbmp {
+
+constexpr int kPsdBlock = 16;
+
+// Stage 1 (psd_export_kernels.cu:12-55): crop box [x0,x1) x [y0,y1) of each
+// primitive's scaled square of half extent 1.5 r, clipped to the canvas; an
+// empty box becomes (0,0,1,1).
+__global__ void psd_bbox_kernel(const float* __restrict__ means2D, const float* __restrict__ radii, int N, int H,
+                                int W, float scale, int* __restrict__ bbox, int* __restrict__ sizes) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const float x = means2D[n * 2 + 0] * scale;
+  const float y = means2D[n * 2 + 1] * scale;
+  const float r = radii[n] * scale;
+  const float half_extent = r * 1.5f;
+  const int x0 = max(0, (int)floorf(x - half_extent));
+  const int y0 = max(0, (int)floorf(y - half_extent));
+  const int x1 = min(W, (int)ceilf(x + half_extent));
+  const int y1 = min(H, (int)ceilf(y + half_extent));
+  int4 b = (x1 <= x0 || y1 <= y0) ? make_int4(0, 0, 1, 1) : make_int4(x0, y0, x1, y1);
+  reinterpret_cast<int4*>(bbox)[n] = b;
+  sizes[2 * n + 0] = b.z - b.x;
+  sizes[2 * n + 1] = b.w - b.y;
+}
+
+// Layout: exclusive prefix sums of layer bytes (w*h*4) and of 16x16 blocks,
+// in one CTA (the reference does the byte sum on the host,
+// psd_export_uint8.py:70-77).  blk has N+1 entries; total_bytes is written.
+__global__ void psd_layout_kernel(const int* __restrict__ sizes, int N, long long* __restrict__ layer_offsets,
+                                  long long* __restrict__ blk, long long* __restrict__ total_bytes) {
+  __shared__ long long s_b[1024], s_k[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int per = (N + nt - 1) / nt;
+  const int lo = min(N, t * per), hi = min(N, lo + per);
+  long long sb = 0, sk = 0;
+  for (int n = lo; n < hi; ++n) {
+    const long long w = sizes[2 * n], h = sizes[2 * n + 1];
+    sb += w * h * 4;
+    sk += ((w + kPsdBlock - 1) / kPsdBlock) * ((h + kPsdBlock - 1) / kPsdBlock);
+  }
+  s_b[t] = sb; s_k[t] = sk;
+  __syncthreads();
+  for (int d = 1; d < nt; d <<= 1) {   // Hillis-Steele inclusive scan
+    const long long vb = t >= d ? s_b[t - d] : 0, vk = t >= d ? s_k[t - d] : 0;
+    __syncthreads();
+    s_b[t] += vb; s_k[t] += vk;
+    __syncthreads();
+  }
+  long long ob = s_b[t] - sb, ok = s_k[t] - sk;
+  for (int n = lo; n < hi; ++n) {
+    const long long w = sizes[2 * n], h = sizes[2 * n + 1];
+    layer_offsets[n] = ob;
+    blk[n] = ok;
+    ob += w * h * 4;
+    ok += ((w + kPsdBlock - 1) / kPsdBlock) * ((h + kPsdBlock - 1) / kPsdBlock);
+  }
+  if (t == nt - 1) {
+    blk[N] = s_k[t];
+    *total_bytes = s_b[t];
+  }
+}
+
+// Template value at canvas pixel (px,py): psd_export_common.h:55-103 (u from
+// (px - x) / r, hard zero when u_t < 0 or u_t >= W-1).
+__device__ __forceinline__ float psd_template_value(const float* __restrict__ tmpl, int t_idx, int P, int Ht, int Wt,
+                                                    int px, int py, float x, float y, float r, float cos_t,
+                                                    float sin_t) {
+  const float u_norm = ((float)px - x) / (r);
+  const float v_norm = ((float)py - y) / (r);
+  const float u_rot = cos_t * u_norm + sin_t * v_norm;
+  const float v_rot = -sin_t * u_norm + cos_t * v_norm;
+  const float u_t = (u_rot + 1.0f) * 0.5f * (Wt - 1);
+  const float v_t = (v_rot + 1.0f) * 0.5f * (Ht - 1);
+  if (u_t < 0.0f || u_t >= Wt - 1 || v_t < 0.0f || v_t >= Ht - 1) return 0.0f;
+  if (t_idx < 0 || t_idx >= P) return 0.0f;   // the reference reads out of bounds here
+  int u0 = (int)floorf(u_t);
+  int v0 = (int)floorf(v_t);
+  u0 = max(0, min(u0, Wt - 1));
+  v0 = max(0, min(v0, Ht - 1));
+  const float wu = u_t - u0;
+  const float wv = v_t - v0;
+  const float wu_inv = 1.0f - wu;
+  const float wv_inv = 1.0f - wv;
+  const float* t = tmpl + (size_t)t_idx * Ht * Wt;
+  const float v00 = t[v0 * Wt + u0];
+  const float v01 = t[v0 * Wt + u0 + 1];
+  const float v10 = t[(v0 + 1) * Wt + u0];
+  const float v11 = t[(v0 + 1) * Wt + u0 + 1];
+  return wu_inv * wv_inv * v00 + wu * wv_inv * v01 + wu_inv * wv * v10 + wu * wv * v11;
+}
+
+// Clamped bilinear of a per-primitive RGB map (psd_export_common.h:124-196),
+// used only with c_blend > 0.
+__device__ __forceinline__ float3 psd_color_map(const float* __restrict__ cm, int map_h, int map_w, float x, float y,
+                                                float radius, float rotation) {
+  float r_inv = radius > 1e-6f ? (1.0f / radius) : 1e6f;
+  float norm_x = x * r_inv;
+  float norm_y = y * r_inv;
+  float cos_theta = cosf(rotation);
+  float sin_theta = sinf(rotation);
+  float rot_x = cos_theta * norm_x + sin_theta * norm_y;
+  float rot_y = -sin_theta * norm_x + cos_theta * norm_y;
+  float coord_x = (rot_x + 1.0f) * 0.5f * (map_w - 1);
+  float coord_y = (rot_y + 1.0f) * 0.5f * (map_h - 1);
+  coord_x = fmaxf(0.0f, fminf(map_w - 1, coord_x));
+  coord_y = fmaxf(0.0f, fminf(map_h - 1, coord_y));
+  int x0 = (int)coord_x;
+  int y0 = (int)coord_y;
+  int x1 = min(x0 + 1, map_w - 1);
+  int y1 = min(y0 + 1, map_h - 1);
+  float fx = coord_x - x0;
+  float fy = coord_y - y0;
+  float3 out;
+  float* o = &out.x;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    const float c00 = cm[3 * (y0 * map_w + x0) + ch], c01 = cm[3 * (y1 * map_w + x0) + ch];
+    const float c10 = cm[3 * (y0 * map_w + x1) + ch], c11 = cm[3 * (y1 * map_w + x1) + ch];
+    const float c0 = c00 * (1.0f - fx) + c10 * fx;
+    const float c1 = c01 * (1.0f - fx) + c11 * fx;
+    o[ch] = c0 * (1.0f - fy) + c1 * fy;
+  }
+  return out;
+}
+
+__device__ __forceinline__ uint8_t to_u8(float v) { return (uint8_t)fmaxf(0.0f, fminf(255.0f, v * 255.0f)); }
+
+struct PsdArgs {
+  int N, P, Ht, Wt;
+  float scale, alpha_max, c_blend;
+};
+
+// Stage 2 (psd_export_kernels.cu:61-198): persistent grid over the 16x16
+// blocks of all crops; block b belongs to the layer n with blk[n] <= b < blk[n+1].
+__global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float* __restrict__ means2D,
+                                                         const float* __restrict__ radii,
+                                                         const float* __restrict__ rot,
+                                                         const float* __restrict__ colors,
+                                                         const float* __restrict__ vis,
+                                                         const float* __restrict__ tmpl, const int* __restrict__ sel,
+                                                         const int* __restrict__ bbox,
+                                                         const long long* __restrict__ layer_offsets,
+                                                         const long long* __restrict__ blk,
+                                                         const float* __restrict__ colors_orig,
+                                                         uint8_t* __restrict__ out) {
+  const long long nblk = blk[a.N];
+  const int lx = threadIdx.x & (kPsdBlock - 1), ly = threadIdx.x / kPsdBlock;
+  for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
+    int lo = 0, hi = a.N;   // largest n with blk[n] <= b
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (blk[mid] <= b) lo = mid; else hi = mid;
+    }
+    const int n = lo;
+    const int4 bb = reinterpret_cast<const int4*>(bbox)[n];
+    const int bw = bb.z - bb.x, bh = bb.w - bb.y;
+    const int bx_n = (bw + kPsdBlock - 1) / kPsdBlock;
+    const long long k = b - blk[n];
+    const int lpx = (int)(k % bx_n) * kPsdBlock + lx, lpy = (int)(k / bx_n) * kPsdBlock + ly;
+    if (lpx >= bw || lpy >= bh) continue;
+    const int px = bb.x + lpx, py = bb.y + lpy;
+    const float x = means2D[n * 2 + 0] * a.scale;
+    const float y = means2D[n * 2 + 1] * a.scale;
+    const float r = radii[n] * a.scale;
+    const float theta = rot[n];
+    const float cos_t = cosf(theta), sin_t = sinf(theta);
+    const float tv = psd_template_value(tmpl, sel[n], a.P, a.Ht, a.Wt, px, py, x, y, r, cos_t, sin_t);
+    const float alpha_val = tv * vis[n] * a.alpha_max;
+    uchar4 px4 = make_uchar4(0, 0, 0, 0);
+    if (!(alpha_val < 0.001f)) {
+      float rgb_r = colors[n * 3 + 0], rgb_g = colors[n * 3 + 1], rgb_b = colors[n * 3 + 2];
+      if (colors_orig != nullptr && a.c_blend > 0.0f) {
+        const float* cm = colors_orig + (size_t)n * a.Ht * a.Wt * 3;
+        const float ux = x / a.scale, uy = y / a.scale;
+        const float upx = (float)px / a.scale, upy = (float)py / a.scale;
+        const float ur = r / a.scale;
+        const float3 co = psd_color_map(cm, a.Ht, a.Wt, upx - ux, upy - uy, ur, theta);
+        rgb_r = (1.0f - a.c_blend) * rgb_r + a.c_blend * co.x;
+        rgb_g = (1.0f - a.c_blend) * rgb_g + a.c_blend * co.y;
+        rgb_b = (1.0f - a.c_blend) * rgb_b + a.c_blend * co.z;
+      }
+      const float mask = tv > 0.0f ? 1.0f : 0.0f;
+      px4 = make_uchar4(to_u8(mask * rgb_r), to_u8(mask * rgb_g), to_u8(mask * rgb_b), to_u8(alpha_val));
+    }
+    *reinterpret_cast<uchar4*>(out + layer_offsets[n] + ((long long)lpy * bw + lpx) * 4) = px4;
+  }
+}
+
+int launch_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale, int* bbox,
+                      int* sizes, cudaStream_t st) {
+  if (N == 0) return DBMP_OK;
+  psd_bbox_kernel<<<(N + 255) / 256, 256, 0, st>>>(means2D, radii, N, H, W, scale, bbox, sizes);
+  DBMP_CHECK_LAUNCH("psd_bbox_kernel");
+  return DBMP_OK;
+}
+
+int launch_psd_layout(const int* sizes, int N, long long* layer_offsets, long long* blk, long long* total,
+                      cudaStream_t st) {
+  psd_layout_kernel<<<1, 1024, 0, st>>>(sizes, N, layer_offsets, blk, total);
+  DBMP_CHECK_LAUNCH("psd_layout_kernel");
+  return DBMP_OK;
+}
+
+int launch_psd_layers(int N, int P, int Ht, int Wt, float scale, float alpha_max, float c_blend,
+                      const float* means2D, const float* radii, const float* rot, const float* colors,
+                      const float* vis, const float* tmpl, const int* sel, const int* bbox,
+                      const long long* layer_offsets, const long long* blk, const float* colors_orig, uint8_t* out,
+                      cudaStream_t st) {
+  if (N == 0) return DBMP_OK;
+  PsdArgs a{N, P, Ht, Wt, scale, alpha_max, c_blend};
+  psd_layers_kernel<<<148 * 8, 256, 0, st>>>(a, means2D, radii, rot, colors, vis, tmpl, sel, bbox, layer_offsets,
+                                             blk, colors_orig, out);
+  DBMP_CHECK_LAUNCH("psd_layers_kernel");
+  return DBMP_OK;
+}
+
+}  // namespace dbmp

@@ -223,6 +223,35 @@ int dbmp_adam_step(const dbmp_canvas* cv, const dbmp_adam_cfg* cfg, const double
                    float* adam_m, float* adam_v, int32_t* step_count, const int32_t* skip_flag,
                    void* stream);
 
+/* PSD stage 1: crop box per primitive, [x0,y0,x1,y1) of the square of half
+ * extent 1.5*r*scale around means2D*scale, clipped to the HxW export canvas;
+ * an empty box becomes (0,0,1,1).  out_bbox (N,4) i32 (16-byte aligned),
+ * out_sizes (N,2) i32 = (w,h).  Bit-identical to the reference.  Replaces
+ * launch_compute_bounding_boxes (cuda_tile_rasterizer/cuda_kernels/
+ * psd_export_kernels.cu:206-231). */
+int dbmp_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale,
+                    int32_t* out_bbox, int32_t* out_sizes, void* stream);
+
+/* PSD layout: layer_offsets (N) i64 = exclusive sum of w*h*4 (byte offset of
+ * each layer in the packed buffer), block_offsets (N+1) i64 = exclusive sum
+ * of 16x16 blocks per layer (scratch for dbmp_psd_layers), *total_bytes
+ * (device i64) = buffer size.  Replaces the host loop of
+ * cuda_tile_rasterizer/psd_export_uint8.py:70-77. */
+int dbmp_psd_layout(const int32_t* sizes, int N, int64_t* layer_offsets, int64_t* block_offsets,
+                    int64_t* total_bytes, void* stream);
+
+/* PSD stage 2: packed uint8 RGBA layers, layer n at byte layer_offsets[n],
+ * row-major over its crop box.  colors / visibility are already sigmoid-ed;
+ * colors_orig (N,Ht,Wt,3) f32 may be null (used only when c_blend > 0).  out
+ * must be 4-byte aligned and hold *total_bytes.  Bytes are identical to the
+ * reference's.  Replaces launch_generate_cropped_layers
+ * (cuda_tile_rasterizer/cuda_kernels/psd_export_kernels.cu:233-273). */
+int dbmp_psd_layers(const float* means2D, const float* radii, const float* rotations,
+                    const float* colors, const float* visibility, const float* templates, int P, int Ht,
+                    int Wt, const int32_t* sel, const int32_t* bbox, const int64_t* layer_offsets,
+                    const int64_t* block_offsets, int N, float scale, float alpha_max, float c_blend,
+                    const float* colors_orig, uint8_t* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

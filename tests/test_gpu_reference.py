@@ -1,0 +1,178 @@
+"""GPU tests against the reference's own CUDA kernels, compiled from the
+reference sources with the reference's flags into oracle/_ref/ (see
+oracle/Makefile).  Skipped when that build is absent.
+
+* PSD export: crop boxes and uint8 RGBA layers bit-identical to
+  psd_export_kernels.cu, with and without colour blending and export scaling.
+* Forward / backward: the reference kernels keep per-pixel caches of K
+  slots and do not guard overflow (tile_forward.cu:219-223), so K is set to
+  the deepest pixel counted by the oracle plus slack, and the caches are
+  sized for it, before the reference kernel is launched.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from oracle import reference_gpu as RG
+from helpers import bin_scene, small_scene
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not RG.available(), reason="reference kernels not built (make -C oracle ref)")]
+
+P_ = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def dev(a, dt=np.float32):
+    return torch.from_numpy(np.ascontiguousarray(a, dt)).cuda()
+
+
+# ---------------------------------------------------------------------------
+# PSD
+def _psd_case(seed, N, H, W, scale, c_blend):
+    rng = np.random.default_rng(seed)
+    from diffbmp_b200 import workloads as wl
+    P, S = 3, 40
+    tm = np.stack([wl.random_shape(rng, S) for _ in range(P)])
+    x = rng.uniform(-10, W / scale + 10, N); y = rng.uniform(-10, H / scale + 10, N)
+    r = np.exp(rng.uniform(np.log(1.5), np.log(0.3 * min(H, W) / scale), N))
+    r[:3] = [1e-3, 0.4, 2.0]                       # degenerate and tiny crops
+    th = rng.uniform(-7, 7, N)
+    v = 1 / (1 + np.exp(-rng.normal(0, 2, N)))
+    c = 1 / (1 + np.exp(-rng.normal(0, 2, (N, 3))))
+    sel = ((N - 1 - np.arange(N)) % P).astype(np.int32)
+    co = rng.uniform(0, 1, (N, S, S, 3)) if c_blend > 0 else None
+    return tm, np.stack([x, y], 1), r, th, v, c, sel, co
+
+
+@pytest.mark.parametrize("seed,N,H,W,scale,c_blend", [(0, 300, 256, 256, 1.0, 0.0), (1, 200, 200, 136, 2.0, 0.0),
+                                                      (2, 150, 160, 192, 1.0, 0.35), (3, 64, 96, 96, 0.5, 1.0)])
+def test_psd_bit_exact_vs_reference_kernel(seed, N, H, W, scale, c_blend):
+    from diffbmp_b200.psd import export_layers
+    tm, m, r, th, v, c, sel, co = _psd_case(seed, N, H, W, scale, c_blend)
+    P, Ht, Wt = tm.shape
+    t_tm, t_m, t_r, t_th, t_v, t_c = dev(tm), dev(m), dev(r), dev(th), dev(v), dev(c)
+    t_sel = dev(sel, np.int32)
+    t_co = dev(co).view(-1) if co is not None else None
+    buf, bbox, sizes, offs = export_layers(t_tm, t_m, t_r, t_th, t_v, t_c, t_sel, H, W, scale, 0.9, c_blend, t_co)
+    # the reference: its two launchers, offsets from a host prefix sum as in psd_export_uint8.py:70-77
+    L = RG.psd()
+    rb = torch.zeros((N, 4), dtype=torch.int32, device="cuda")
+    rs = torch.zeros((N, 2), dtype=torch.int32, device="cuda")
+    L.launch_compute_bounding_boxes(P_(t_m), P_(t_r), P_(t_th), P_(t_tm), P_(t_sel), P_(rb), P_(rs), N, H, W, Ht, Wt,
+                                    ctypes.c_float(scale), ctypes.c_float(0.9))
+    torch.cuda.synchronize()
+    assert torch.equal(rb, bbox) and torch.equal(rs, sizes)
+    hs = rs.cpu().numpy()
+    ro = np.concatenate([[0], np.cumsum(hs[:, 0].astype(np.int64) * hs[:, 1] * 4)[:-1]]).astype(np.int32)
+    assert np.array_equal(ro, offs.cpu().numpy())
+    total = int((hs[:, 0].astype(np.int64) * hs[:, 1] * 4).sum())
+    rbuf = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    t_ro = dev(ro, np.int32)
+    L.launch_generate_cropped_layers(P_(t_m), P_(t_r), P_(t_th), P_(t_c), P_(t_v), P_(t_tm), P_(t_sel), P_(rb),
+                                     P_(t_ro), P_(rbuf), N, H, W, Ht, Wt, ctypes.c_float(scale),
+                                     ctypes.c_float(0.9), ctypes.c_float(c_blend), P_(t_co), W, H)
+    torch.cuda.synchronize()
+    neq = (rbuf != buf).nonzero().flatten().cpu().numpy()
+    where = []
+    for b in neq[:4]:
+        n = int(np.searchsorted(ro, b, side="right") - 1)
+        k = int(b - ro[n]); w = int(hs[n, 0])
+        where.append((n, (k // 4) % w, (k // 4) // w, k % 4, int(rbuf[b]), int(buf[b])))
+    assert len(neq) == 0, f"{len(neq)} of {total} bytes differ from the reference kernel: " \
+                          f"(layer, x, y, channel, reference, ours) {where}"
+
+
+def test_psd_vs_oracle():
+    """Against the FP64 restatement: equal except where float rounding of the
+    reference's fast-math path can move a value across a truncation step."""
+    from diffbmp_b200.psd import export_layers
+    tm, m, r, th, v, c, sel, co = _psd_case(7, 200, 200, 240, 1.0, 0.0)
+    buf, bbox, sizes, offs = export_layers(dev(tm), dev(m), dev(r), dev(th), dev(v), dev(c), dev(sel, np.int32), 200,
+                                           240, 1.0, 0.9)
+    bb, sz = O.psd_bboxes(m, r, 200, 240, 1.0)
+    assert np.array_equal(bb, bbox.cpu().numpy()) and np.array_equal(sz, sizes.cpu().numpy())
+    ref, amb = O.psd_layers(m, r, th, c, v, tm, sel, bb, offs.cpu().numpy(), 1.0, 0.9)
+    ours = buf.cpu().numpy().astype(np.int32)
+    d = np.abs(ours - ref.astype(np.int32))
+    assert d[amb == 0].max(initial=0) == 0
+    assert d.max(initial=0) <= 1
+    print("ambiguous bytes:", int(amb.sum()), "of", amb.size, "differing:", int((d > 0).sum()))
+
+
+# ---------------------------------------------------------------------------
+# forward / backward
+def _run_reference(sc: O.Scene, offs, idx):
+    f = O.forward(sc, offs, idx)
+    K = f["stats"]["max_depth"] + 16
+    H, W, N = sc.H, sc.W, sc.N
+    P, Ht, Wt = sc.templates.shape
+    caches = torch.zeros(5 * H * W * K + 8 * K, dtype=torch.float32, device="cuda")
+    counts = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+    sig = torch.zeros(8 * N + 8, dtype=torch.float32, device="cuda")
+    d = dict(m=dev(sc.means2D), r=dev(sc.radii), th=dev(sc.rot), v=dev(sc.opac), c=dev(sc.colors),
+             t=dev(sc.templates), s=dev(sc.sel, np.int32), o=dev(offs, np.int32), i=dev(np.maximum(idx, 0), np.int32))
+    color = torch.zeros((H, W, 3), device="cuda")
+    alpha = torch.zeros((H, W), device="cuda")
+    Lr = RG.raster()
+    rc = Lr.ref_forward(H, W, sc.ts, ctypes.c_float(sc.alpha_max), N, P, Ht, Wt, K, P_(d["m"]), P_(d["r"]),
+                        P_(d["th"]), P_(d["v"]), P_(d["c"]), P_(d["t"]), P_(d["s"]), P_(d["o"]), len(offs),
+                        P_(d["i"]), len(idx), P_(color), P_(alpha), P_(caches), P_(counts), P_(sig))
+    assert rc == 0
+    return color, alpha, (d, caches, counts, sig, K), f
+
+
+@pytest.mark.parametrize("name,ts", [("c0", 32), ("atlas", 16)])
+def test_forward_backward_vs_reference_kernels(name, ts):
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.rasterizer import Atlas, Rasterizer
+    if name == "c0":
+        s = wl.make_scene("c0", 2)
+    else:
+        s = wl.make_scene("c1", 3, H=160, W=192, N=300)
+    sc = O.Scene(s.H, s.W, ts, s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.templates, s.sel)
+    offs, idx = bin_scene(sc)
+    rcol, ralp, rstate, fo = _run_reference(sc, offs, idx)
+    rz = Rasterizer(sc.H, sc.W, ts, t_stop=1e-7)
+    d = rstate[0]
+    atlas = Atlas(d["t"])
+    col, alp, state = rz.forward(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], atlas)
+    torch.cuda.synchronize()
+    e_ref = np.abs(rcol.cpu().numpy() - fo["color"]).max()
+    e_ours = np.abs(col.cpu().numpy() - fo["color"]).max()
+    band, _ = O.boundary_band(sc, offs, idx, edge=1e-3)
+    diff = np.abs(col.cpu().numpy() - rcol.cpu().numpy()).max(-1)
+    print(f"{name}: max err vs FP64 oracle: reference {e_ref:.2e}, ours {e_ours:.2e}; "
+          f"ours vs reference outside band {diff[band == 0].max(initial=0):.2e}")
+    # the reference's own fast-math error against FP64 bounds how close two correct kernels can be
+    assert diff[band == 0].max(initial=0) <= max(2e-5, 2 * e_ref)
+
+    rng = np.random.default_rng(4)
+    gc = rng.normal(0, 1, (sc.H, sc.W, 3)).astype(np.float32)
+    ga = rng.normal(0, 1, (sc.H, sc.W)).astype(np.float32)
+    d, caches, counts, sig, K = rstate
+    N = sc.N
+    P, Ht, Wt = sc.templates.shape
+    rg = [torch.zeros(sh, device="cuda") for sh in ((N, 2), (N,), (N,), (N,), (N, 3))]
+    t_gc, t_ga = dev(gc), dev(ga)        # keep them referenced while the kernels read them
+    rc = RG.raster().ref_backward(sc.H, sc.W, ts, ctypes.c_float(1.0), N, P, Ht, Wt, K, P_(d["m"]), P_(d["r"]),
+                                  P_(d["th"]), P_(d["v"]), P_(d["c"]), P_(d["t"]), P_(d["s"]), P_(d["o"]), len(offs),
+                                  P_(d["i"]), len(idx), P_(t_gc), P_(t_ga), P_(caches), P_(counts), P_(sig),
+                                  *[P_(t) for t in rg])
+    assert rc == 0
+    ours = rz.backward(state, t_gc, t_ga, d["r"], d["th"], d["v"], d["c"], atlas)
+    refo = O.backward(sc, offs, idx, gc, ga)
+    rgn = np.concatenate([t.cpu().numpy().reshape(N, -1) for t in rg], 1)
+    ogn = np.concatenate([t.cpu().numpy().reshape(N, -1) for t in ours], 1)
+    hi = O.backward(sc, offs, idx, gc, ga, edge=1e-3)
+    lo = O.backward(sc, offs, idx, gc, ga, edge=-1e-3)
+    for k in range(8):
+        nrm = np.linalg.norm(refo[:, k])
+        e_r = np.linalg.norm(rgn[:, k] - refo[:, k]) / nrm
+        e_o = np.linalg.norm(ogn[:, k] - refo[:, k]) / nrm
+        e_ro = np.linalg.norm(ogn[:, k] - rgn[:, k]) / nrm
+        spread = np.linalg.norm(hi[:, k] - lo[:, k]) / nrm
+        print(f"  block {k}: reference {e_r:.2e}, ours {e_o:.2e}, ours vs reference {e_ro:.2e}, band {spread:.2e}")
+        assert e_ro <= max(1e-4, 2 * e_r) + spread
