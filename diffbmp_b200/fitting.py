@@ -44,9 +44,10 @@ class FitConfig:
     headroom: float = 1.3
 
 
-def _dev_f32(a, device):
+def _dev_f32(a, device, copy=True):
     if isinstance(a, torch.Tensor):
-        return a.detach().to(device=device, dtype=torch.float32).contiguous().clone()
+        t = a.detach().to(device=device, dtype=torch.float32).contiguous()
+        return t.clone() if copy and t.data_ptr() == a.data_ptr() else t
     return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(device)
 
 
@@ -66,9 +67,10 @@ class ImageFitter:
         self.sel = (sel if isinstance(sel, torch.Tensor) else torch.from_numpy(np.asarray(sel))).to(
             device=dev, dtype=torch.int32).contiguous()
         self.N = int(self.radii.numel())
-        self.target = _dev_f32(target, dev)
+        # read-only images: no private copy is needed
+        self.target = _dev_f32(target, dev, copy=False)
         self.H, self.W = int(self.target.shape[0]), int(self.target.shape[1])
-        self.background = _dev_f32(background, dev) if background is not None else None
+        self.background = _dev_f32(background, dev, copy=False) if background is not None else None
         self.atlas = atlas
         self.rz = Rasterizer(self.H, self.W, cfg.tile_size, cfg.alpha_max, cfg.t_stop, device=dev)
         self.cv = self.rz.canvas(self.N, atlas)

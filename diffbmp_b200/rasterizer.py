@@ -168,11 +168,14 @@ class Rasterizer:
         for _ in range(3):
             self._ensure(cv, self.capacity)
             ws, wsb = self._ws_ptr()
-            call("dbmp_bin", ctypes.byref(cv), *args, _ptr(self._idx), ctypes.c_longlong(self.capacity),
+            # each binning owns its index list: a ForwardState must stay valid
+            # while later forwards on this canvas run (batch APIs keep several)
+            indices = torch.empty(max(self.capacity, 1), dtype=torch.int32, device=self.device)
+            call("dbmp_bin", ctypes.byref(cv), *args, _ptr(indices), ctypes.c_longlong(self.capacity),
                  _ptr(self._small), ctypes.c_void_p(self._small.data_ptr() + 4), ws, ctypes.c_size_t(wsb), st)
             L, overflow = self._small.tolist()
             if not overflow:
-                return prim_info, TileLists(offsets, self._idx, int(L))
+                return prim_info, TileLists(offsets, indices, int(L))
             self._ensure(cv, int(L * 1.25) + 4096)
         raise DbmpError("binning capacity did not converge")
 

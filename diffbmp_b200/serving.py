@@ -1,0 +1,209 @@
+"""Continuous-batching server for fit-an-image jobs.
+
+Replaces the reference's only batching -- a host loop calling the single-image
+forward/backward once per candidate (cuda_tile_rasterizer/tile_rasterize.cu:500-636,
+simple_tile_renderer.py:268-429) -- with a request loop:
+
+* jobs arrive over time (``JobRequest.arrival`` seconds after start) and are
+  admitted into a slot as soon as a slot is free and their estimated device
+  memory fits the HBM budget;
+* an admitted job stays resident in HBM (``ImageFitter``: parameters, Adam
+  moments, target, tile lists, scratch) and its fit iteration (binning, fused
+  forward + L2 + backward, Adam) is captured once in a CUDA graph;
+* every active job advances independently on its own stream of a pool, at
+  most ``depth`` iterations ahead of the host, so iterations of small and
+  large canvases overlap on the device instead of waiting for each other;
+* a job retires when its device step counter reaches its iteration count;
+  list-capacity overflows are detected there and the skipped iterations are
+  replayed (exact results);
+* latency = retirement time - arrival time; throughput = retired jobs over
+  the span from the first arrival to the last retirement.
+"""
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from .fitting import FitConfig, ImageFitter
+from .rasterizer import Atlas
+
+
+@dataclass
+class JobRequest:
+    job_id: int
+    arrival: float               # seconds after the server starts
+    spec: object                 # workloads.SceneSpec
+    iterations: int = 100
+
+
+@dataclass
+class JobResult:
+    job_id: int
+    arrival: float
+    admitted: float
+    done: float
+    loss: float
+    replayed: int
+    params: Optional[dict] = None
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def estimate_bytes(spec, tile_size=32) -> int:
+    """Upper estimate of one job's resident device memory: target and
+    background images, per-pixel state, and tile lists sized as if every
+    primitive covered the tiles of its largest square (1.3x headroom, plus the
+    binning scratch of ~4 words per entry)."""
+    H, W, N = spec.H, spec.W, spec.N
+    T = ((H + tile_size - 1) // tile_size) * ((W + tile_size - 1) // tile_size)
+    r = np.asarray(spec.radii, np.float64)
+    side = np.minimum(np.ceil(2.0 * r / tile_size) + 2.0, max(H, W) / tile_size + 1)
+    L = float(np.minimum(side * side, T).sum()) * 1.3 + 4096
+    return int(2 * H * W * 12 + H * W * 8 + L * 4 * 5 + N * 512 + (T + 1) * 4)
+
+
+@dataclass
+class _Slot:
+    req: JobRequest
+    fitter: ImageFitter
+    stream: torch.cuda.Stream
+    admitted: float
+    issued: int = 0
+    events: collections.deque = field(default_factory=collections.deque)
+    nbytes: int = 0
+
+
+class Server:
+    """Request loop over a shared atlas.  ``kind``: atlas storage ("f16" for
+    the precision form, "f32" plain); ``fused``: fused fwd/bwd kernel."""
+
+    def __init__(self, atlas_templates: torch.Tensor, kind="f16", fused=True, max_slots=48,
+                 hbm_budget=150e9, n_streams=16, depth=2, graphs=True, lr=0.01, keep_params=False):
+        self.atlas = Atlas(atlas_templates, kind)
+        self.cfg = FitConfig(lr=lr, fused=fused)
+        self.max_slots = max_slots
+        self.budget = float(hbm_budget)
+        self.streams = [torch.cuda.Stream() for _ in range(n_streams)]
+        self.depth = depth
+        self.graphs = graphs
+        self.keep_params = keep_params
+
+    def _admit(self, req: JobRequest, now: float, stream) -> _Slot:
+        s = req.spec
+        stream.wait_stream(torch.cuda.default_stream())   # job tensors may come from the default stream
+        with torch.cuda.stream(stream):
+            f = ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, self.atlas, s.target,
+                            s.background, self.cfg)
+            if self.graphs:
+                f.capture()
+        return _Slot(req, f, stream, now)
+
+    def run(self, requests: List[JobRequest], realtime=True) -> List[JobResult]:
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        active: List[_Slot] = []
+        results: List[JobResult] = []
+        used = 0
+        t0 = time.perf_counter()
+        clock = lambda: time.perf_counter() - t0
+        rr = 0
+        while pending or active:
+            now = clock()
+            # admission: arrived jobs, while slots and the HBM budget allow
+            while pending and (pending[0].arrival <= now or not realtime) and len(active) < self.max_slots:
+                est = estimate_bytes(pending[0].spec, self.cfg.tile_size)
+                if used + est > self.budget and active:
+                    break
+                req = pending.popleft()
+                slot = self._admit(req, max(now, req.arrival) if realtime else now, self.streams[rr % len(self.streams)])
+                rr += 1
+                slot.nbytes = est
+                used += est
+                active.append(slot)
+            progressed = False
+            for slot in list(active):
+                # retire finished iterations
+                while slot.events and slot.events[0].query():
+                    slot.events.popleft()
+                    progressed = True
+                f = slot.fitter
+                if slot.issued >= slot.req.iterations and not slot.events:
+                    replayed = 0
+                    with torch.cuda.stream(slot.stream):
+                        replayed = f.sync()
+                        loss = f.loss()
+                    params = {k: v.detach().clone() for k, v in f.params().items()} if self.keep_params else None
+                    results.append(JobResult(slot.req.job_id, slot.req.arrival, slot.admitted, clock(), loss,
+                                             replayed, params))
+                    active.remove(slot)
+                    used -= slot.nbytes
+                    progressed = True
+                    continue
+                # issue up to `depth` iterations ahead of the host
+                while slot.issued < slot.req.iterations and len(slot.events) < self.depth:
+                    with torch.cuda.stream(slot.stream):
+                        f.step()
+                        ev = torch.cuda.Event()
+                        ev.record(slot.stream)
+                    slot.events.append(ev)
+                    slot.issued += 1
+                    progressed = True
+            if not progressed:
+                if active:
+                    # nothing to issue: wait for the oldest in-flight iteration
+                    oldest = min((s for s in active if s.events), key=lambda s: s.issued, default=None)
+                    if oldest is not None:
+                        oldest.events[0].synchronize()
+                    else:
+                        time.sleep(0.0002)
+                elif pending and realtime:
+                    time.sleep(max(0.0, min(0.002, pending[0].arrival - clock())))
+        torch.cuda.synchronize()
+        return results
+
+
+def poisson_requests(n, rate, atlas, seed=0, iterations=100, sizes=(256, 512, 1024, 2048), n_range=(256, 20000),
+                     device=None):
+    """n jobs of the serving workload, exponential inter-arrival times at `rate`
+    jobs/s, drawn from the shared atlas (targets built on `device` if given)."""
+    from . import workloads as wl
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        reqs.append(JobRequest(i, t, wl.make_job(rng, atlas, sizes, n_range, device), iterations))
+    return reqs
+
+
+def summarize(results: List[JobResult]):
+    lat = np.array([r.latency for r in results])
+    span = max(r.done for r in results) - min(r.arrival for r in results)
+    return dict(jobs=len(results), jobs_per_s=len(results) / span, p50_s=float(np.percentile(lat, 50)),
+                p99_s=float(np.percentile(lat, 99)), mean_loss=float(np.mean([r.loss for r in results])),
+                replayed=int(sum(r.replayed for r in results)))
+
+
+def run_sequential(requests: List[JobRequest], atlas_templates, kind="f32", fused=False, lr=0.01, graphs=False):
+    """One job at a time, to completion: the plain baseline of the serving target."""
+    atlas = Atlas(atlas_templates, kind)
+    cfg = FitConfig(lr=lr, fused=fused)
+    out = []
+    t0 = time.perf_counter()
+    for req in requests:
+        s = req.spec
+        f = ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, atlas, s.target,
+                        s.background, cfg)
+        if graphs:
+            f.capture()
+        for _ in range(req.iterations):
+            f.step()
+        rep = f.sync()
+        out.append(JobResult(req.job_id, 0.0, 0.0, time.perf_counter() - t0, f.loss(), rep))
+    return out, time.perf_counter() - t0

@@ -67,20 +67,26 @@ def random_shape(rng: np.random.Generator, size: int) -> np.ndarray:
 def smooth_field(rng: np.random.Generator, H: int, W: int, n: int = 8,
                  noise: float = 0.0) -> np.ndarray:
     """(H,W,3) sum of n random 2-D sinusoids per channel, rescaled to [0,1]."""
-    yy, xx = np.mgrid[0:H, 0:W].astype(np.float64)
-    out = np.zeros((H, W, 3), np.float64)
+    xs = np.arange(W, dtype=np.float64)
+    ys = np.arange(H, dtype=np.float64)
+    out = np.zeros((H, W, 3), np.float32)
     for ch in range(3):
-        f = np.zeros((H, W))
-        for _ in range(n):
+        # sum_k a_k sin(u_k + v_k) = sum_k a_k (cos v_k sin u_k + sin v_k cos u_k), one (H,2n)@(2n,W) product
+        A = np.zeros((H, 2 * n)); B = np.zeros((2 * n, W))
+        for k in range(n):
             fx, fy = rng.uniform(-4, 4, 2)
             ph = rng.uniform(0, 2 * np.pi)
             a = rng.uniform(0.5, 1.0)
-            f += a * np.sin(2 * np.pi * (fx * xx / W + fy * yy / H) + ph)
+            u = 2 * np.pi * fx * xs / W + ph
+            v = 2 * np.pi * fy * ys / H
+            A[:, 2 * k], A[:, 2 * k + 1] = a * np.cos(v), a * np.sin(v)
+            B[2 * k], B[2 * k + 1] = np.sin(u), np.cos(u)
+        f = (A @ B).astype(np.float32)
         f -= f.min()
-        f /= max(f.max(), 1e-12)
+        f /= max(float(f.max()), 1e-12)
         out[..., ch] = f
     if noise > 0:
-        out += rng.normal(0.0, noise, out.shape)
+        out += noise * rng.standard_normal(out.shape, dtype=np.float32)
     return out.astype(np.float32)
 
 
@@ -154,15 +160,46 @@ def make_scene(config: str, seed: int = 0, **over) -> SceneSpec:
                      alpha_max=over.get("alpha_max", 1.0), meta=dict(config=config, seed=seed))
 
 
+def smooth_field_device(rng: np.random.Generator, H: int, W: int, device, n: int = 8, noise: float = 0.0):
+    """smooth_field built on a torch device (same construction, float32)."""
+    import torch
+    xs = torch.arange(W, dtype=torch.float32, device=device)
+    ys = torch.arange(H, dtype=torch.float32, device=device)
+    chans = []
+    for _ in range(3):
+        p = rng.uniform(size=(n, 4))
+        fx, fy = -4 + 8 * p[:, 0], -4 + 8 * p[:, 1]
+        ph, a = 2 * np.pi * p[:, 2], 0.5 + 0.5 * p[:, 3]
+        t = lambda z: torch.tensor(z, dtype=torch.float32, device=device)
+        u = 2 * np.pi * t(fx)[:, None] * xs[None] / W + t(ph)[:, None]          # (n, W)
+        v = 2 * np.pi * t(fy)[:, None] * ys[None] / H                           # (n, H)
+        A = torch.cat([t(a)[:, None] * torch.cos(v), t(a)[:, None] * torch.sin(v)], 0).T   # (H, 2n)
+        B = torch.cat([torch.sin(u), torch.cos(u)], 0)                          # (2n, W)
+        f = A @ B
+        f = f - f.min()
+        chans.append(f / f.max().clamp_min(1e-12))
+    out = torch.stack(chans, -1)
+    if noise > 0:
+        g = torch.Generator(device=device).manual_seed(int(rng.integers(0, 2**62)))
+        out += noise * torch.randn(out.shape, generator=g, device=device)
+    return out.contiguous()
+
+
 def make_job(rng: np.random.Generator, atlas: np.ndarray, sizes=(256, 512, 1024, 2048),
-             n_range=(256, 20000)) -> SceneSpec:
+             n_range=(256, 20000), device=None) -> SceneSpec:
     """One serving job: W and H drawn independently from `sizes`, N log-uniform
-    in n_range, primitives drawn from the shared atlas."""
+    in n_range, primitives drawn from the shared atlas.  With `device` the
+    target and background are built there as torch tensors."""
     H = int(rng.choice(sizes)); W = int(rng.choice(sizes))
     N = int(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]))))
     P = atlas.shape[0]
     means2D, r, th, v, c, sel = sample_params(rng, H, W, N, P, "uniform")
-    target = smooth_field(rng, H, W, noise=0.02)
-    bg = np.ones((H, W, 3), np.float32)
+    if device is not None:
+        import torch
+        target = smooth_field_device(rng, H, W, device, noise=0.02)
+        bg = torch.ones((H, W, 3), dtype=torch.float32, device=device)
+    else:
+        target = smooth_field(rng, H, W, noise=0.02)
+        bg = np.ones((H, W, 3), np.float32)
     return SceneSpec(H, W, N, means2D, r, th, v, c, atlas, sel, target, bg,
                      meta=dict(config="c4"))
