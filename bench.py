@@ -216,7 +216,7 @@ def counts(job, torch):
     import ctypes
     from diffbmp_b200._lib import call
     from diffbmp_b200.rasterizer import _ptr, _stream
-    c = torch.zeros(6, dtype=torch.int64, device="cuda")
+    c = torch.zeros(7, dtype=torch.int64, device="cuda")
     call("dbmp_count", ctypes.byref(job.cv), _ptr(job.prim_info), _ptr(job.atlas.data), _ptr(job.offsets),
          _ptr(job.rz._idx), _ptr(c), _stream())
     return [int(v) for v in c.tolist()]
@@ -384,7 +384,7 @@ def main():
              _ptr(job.loss_dev), None, _stream())
     job._enqueue(); torch.cuda.synchronize()
     t_kernel = kernel_time(job, fused_launch, max(5, args.steps // 4), torch)
-    cand, frag, L, went, slots, miss = counts(job, torch)
+    cand, frag, L, went, slots, miss, _ = counts(job, torch)
     flop = 12.0 * cand + 144.0 * frag
     fp32_peak = fp32_simt_peak_tflops(torch)
     achieved = flop / t_kernel / 1e12

@@ -211,11 +211,16 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
 int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
                const int32_t* tile_indices, unsigned long long* counts, void* stream) {
   Geom g;
-  int rc = make_geom(cv, &g, "dbmp_count");
+  // t_stop = 0 is allowed here: counting without termination (every fragment)
+  dbmp_canvas c2 = cv ? *cv : dbmp_canvas{};
+  const bool no_stop = cv && cv->t_stop == 0.f;
+  if (no_stop) c2.t_stop = 0.5f;
+  int rc = make_geom(cv ? &c2 : nullptr, &g, "dbmp_count");
   if (rc) return rc;
+  if (no_stop) g.t_stop = 0.f;
   REQUIRE(atlas && tile_offsets && tile_indices && counts, "dbmp_count: null pointer");
   REQUIRE(g.N == 0 || prim_info, "dbmp_count: prim_info is null");
-  cudaError_t e = cudaMemsetAsync(counts, 0, 6 * sizeof(unsigned long long), (cudaStream_t)stream);
+  cudaError_t e = cudaMemsetAsync(counts, 0, 7 * sizeof(unsigned long long), (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(counts)");
   return launch_count(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, counts,
                       (cudaStream_t)stream);

@@ -166,6 +166,9 @@ struct TileWalker {
                                           float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP],
                                           unsigned long long* cnt = nullptr) {
     unsigned long long n_cand = 0, n_frag = 0, n_went = 0, n_slots = 0, n_miss = 0;
+    unsigned n_depth[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) n_depth[p] = 0;
     bool live[NP];
     bool all_done = true;
 #pragma unroll
@@ -228,7 +231,7 @@ struct TileWalker {
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
             const bool frag = s[p].ok && m[p] > 1e-6f;
-            if (STATS) n_frag += frag;
+            if (STATS) { n_frag += frag; n_depth[p] += frag; }
             if (__any_sync(0xffffffffu, frag)) {
               const float a = frag ? g2.x * m[p] : 0.f;
               const float w = T[p] * a;
@@ -250,10 +253,15 @@ struct TileWalker {
     if (STATS) {
       atomicAdd(cnt + 0, n_cand);
       atomicAdd(cnt + 1, n_frag);
+      unsigned dmax = 0;
+#pragma unroll
+      for (int p = 0; p < NP; ++p) dmax = max(dmax, n_depth[p]);
+      dmax = __reduce_max_sync(0xffffffffu, dmax);
       if (lane == 0) {
         atomicAdd(cnt + 3, n_went);
         atomicAdd(cnt + 4, n_slots);
         atomicAdd(cnt + 5, n_miss);
+        atomicMax(cnt + 6, (unsigned long long)dmax);
       }
     }
   }

@@ -177,9 +177,11 @@ int dbmp_backward_noalloc_max_prims(void);
  * pixel terminates, counts[1] = fragments composited, counts[2] = tile-list
  * entries (sum over tiles), counts[3] = (warp, entry) pairs a warp evaluated,
  * counts[4] = pixel slots still running summed over those pairs, counts[5] =
- * (warp, entry) pairs rejected by the warp-footprint test.  counts: 6 device
- * u64, zeroed by the call.  Used for roofline accounting and load analysis;
- * no reference counterpart. */
+ * (warp, entry) pairs rejected by the warp-footprint test, counts[6] = the
+ * largest number of fragments composited at one pixel.  cv->t_stop may be 0
+ * here to count without termination (every fragment, as the reference
+ * composites).  counts: 7 device u64, zeroed by the call.  Used for roofline
+ * and memory accounting; no reference counterpart. */
 int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
                const int32_t* tile_offsets, const int32_t* tile_indices,
                unsigned long long* counts, void* stream);
