@@ -216,7 +216,7 @@ def counts(job, torch):
     import ctypes
     from diffbmp_b200._lib import call
     from diffbmp_b200.rasterizer import _ptr, _stream
-    c = torch.zeros(7, dtype=torch.int64, device="cuda")
+    c = torch.zeros(10, dtype=torch.int64, device="cuda")
     call("dbmp_count", ctypes.byref(job.cv), _ptr(job.prim_info), _ptr(job.atlas.data), _ptr(job.offsets),
          _ptr(job.rz._idx), _ptr(c), _stream())
     return [int(v) for v in c.tolist()]
@@ -384,7 +384,7 @@ def main():
              _ptr(job.loss_dev), None, _stream())
     job._enqueue(); torch.cuda.synchronize()
     t_kernel = kernel_time(job, fused_launch, max(5, args.steps // 4), torch)
-    cand, frag, L, went, slots, miss, _ = counts(job, torch)
+    cand, frag, L, went, slots, miss, _, empty, clear, bad = counts(job, torch)
     flop = 12.0 * cand + 144.0 * frag
     fp32_peak = fp32_simt_peak_tflops(torch)
     achieved = flop / t_kernel / 1e12
@@ -415,7 +415,8 @@ def main():
                      "kernel": "fused_kernel<32, F16_PAIR>", "kernel_ms": t_kernel * 1e3,
                      "flop_model": "12*C + 144*F_live (C pairs passing cull, F_live fragments composited)",
                      "C": cand, "F_live": frag, "warp_entries": went, "live_pixel_slots": slots,
-                     "footprint_rejects": miss,
+                     "footprint_rejects": miss, "empty_warp_entries": empty, "grid_skips": clear,
+                     "grid_skips_with_fragment": bad,
                      "peak_source": "measured in-run: cuBLAS SGEMM 8192^3, TF32 off (FP32 SIMT pipe)",
                      "hbm_peak_gbs_measured": peaks.get("hbm_gbs")},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d,

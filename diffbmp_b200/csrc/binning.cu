@@ -166,7 +166,15 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
   pi.cb = sigmoid_precise(colors[3 * n + 2]);
   const bool nan_geom = isnan(pi.a00) || isnan(pi.a01) || isnan(pi.a10) || isnan(pi.a11) || isnan(mx) || isnan(my);
   pi.toff = !valid ? kNoFrag : (nan_geom ? kSolid : tid * template_records(g.kind, g.Ht, g.Wt));
-  pi.rinv = (float)rinv; pi.cs = (float)c; pi.sn = (float)s;
+  // clearance a warp footprint needs before the walk may skip it: the
+  // footprint's texel-space half extent, plus the bilinear reach of 1 texel,
+  // plus slack for the rounding of the per-pixel texel coordinates
+  const float ex = fabsf(pi.a00) * g.fhx + fabsf(pi.a01) * g.fhy;
+  const float ey = fabsf(pi.a10) * g.fhx + fabsf(pi.a11) * g.fhy;
+  const float need = fmaxf(ex, ey) + 1.05f;
+  pi.goff = valid ? tid * g.gGx * g.gGy : 0;
+  pi.gext = (atlas_has_grid(g.kind) && need < (float)kGridCap) ? (int)ceilf(need) : kGridCap + 1;
+  pi.pad = 0;
   out[n] = pi;
 
   if (rects == nullptr) return;
@@ -317,14 +325,59 @@ int launch_template_bboxes(const float* tmpl, int P, int Ht, int Wt, float* out,
 }
 
 size_t atlas_bytes(int P, int Ht, int Wt, int kind) {
-  const size_t recs = (size_t)P * template_records(kind, Ht, Wt);
-  switch (kind) {
-    case ATLAS_F32: return recs * 4;
-    case ATLAS_F32_QUAD: return recs * 16;
-    case ATLAS_F16_QUAD: case ATLAS_BF16_QUAD: return recs * 8;
-    case ATLAS_F16_PAIR: case ATLAS_BF16_PAIR: return recs * 4;
-    default: return 0;
+  if (kind < ATLAS_F32 || kind > ATLAS_BF16_PAIR) return 0;
+  if (!atlas_has_grid(kind)) return atlas_record_bytes(P, Ht, Wt, kind);
+  int sx, sy, gx, gy;
+  grid_shape(Wt, &sx, &gx);
+  grid_shape(Ht, &sy, &gy);
+  return atlas_grid_offset(P, Ht, Wt, kind) + (size_t)P * gx * gy;
+}
+
+// Clearance grid (layout in dbmp_internal.cuh), one CTA per (cell column,
+// template).  Separable: per template row the x-distance from the column's
+// range to the nearest support texel of that row, then per cell the minimum
+// over rows of max(row distance, y-distance).  Texels further than kGridCap-1
+// beyond the cell cannot lower a capped value and are not visited.
+__global__ void atlas_grid_kernel(const float* __restrict__ tmpl, int Ht, int Wt, int gsx, int gsy, int Gx, int Gy,
+                                  unsigned char* __restrict__ grid) {
+  extern __shared__ unsigned char s_row[];   // Ht row distances
+  const int ix = blockIdx.x, p = blockIdx.y;
+  const float* t = tmpl + (size_t)p * Ht * Wt;
+  const int lo = ix << gsx, hi = min((ix + 1) << gsx, Wt - 1);
+  const int xa = max(0, lo - (kGridCap - 1)), xb = min(Wt - 1, hi + (kGridCap - 1));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int y = warp; y < Ht; y += nwarps) {
+    int best = kGridCap;
+    const float* row = t + (size_t)y * Wt;
+    for (int x = xa + lane; x <= xb; x += 32) {
+      const float v = row[x];
+      if (!(v <= kGridSupport)) best = min(best, max(0, max(lo - x, x - hi)));
+    }
+    best = __reduce_min_sync(0xffffffffu, best);
+    if (lane == 0) s_row[y] = (unsigned char)best;
   }
+  __syncthreads();
+  for (int iy = threadIdx.x; iy < Gy; iy += blockDim.x) {
+    const int ylo = iy << gsy, yhi = min((iy + 1) << gsy, Ht - 1);
+    const int ya = max(0, ylo - (kGridCap - 1)), yb = min(Ht - 1, yhi + (kGridCap - 1));
+    int best = kGridCap;
+    for (int y = ya; y <= yb; ++y) best = min(best, max((int)s_row[y], max(0, max(ylo - y, y - yhi))));
+    grid[((size_t)p * Gy + iy) * Gx + ix] = (unsigned char)best;
+  }
+}
+
+int launch_atlas_grid(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st) {
+  int sx, sy, gx, gy;
+  grid_shape(Wt, &sx, &gx);
+  grid_shape(Ht, &sy, &gy);
+  unsigned char* grid = static_cast<unsigned char*>(out) + atlas_grid_offset(P, Ht, Wt, kind);
+  if (Ht > 48 * 1024) {   // row distances do not fit the shared buffer: clearance 0 never skips
+    cudaError_t e = cudaMemsetAsync(grid, 0, (size_t)P * gx * gy, st);
+    return e == cudaSuccess ? DBMP_OK : cuda_status(e, "cudaMemsetAsync(grid)");
+  }
+  atlas_grid_kernel<<<dim3(gx, P), 256, Ht, st>>>(tmpl, Ht, Wt, sx, sy, gx, gy, grid);
+  DBMP_CHECK_LAUNCH("atlas_grid_kernel");
+  return DBMP_OK;
 }
 
 int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st) {
@@ -337,10 +390,10 @@ int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* 
     case ATLAS_F32_QUAD: atlas_pack_kernel<float><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (float*)out); break;
     case ATLAS_F16_QUAD: atlas_pack_kernel<__half><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (__half*)out); break;
     case ATLAS_BF16_QUAD: atlas_pack_kernel<__nv_bfloat16><<<blocks, 256, 0, st>>>(tmpl, P, Ht, Wt, (__nv_bfloat16*)out); break;
-    default: set_error("dbmp_atlas_pack: kind %d is not a quad kind", kind); return DBMP_ERR_INVALID;
+    default: set_error("dbmp_atlas_pack: kind %d is not a packed kind", kind); return DBMP_ERR_INVALID;
   }
   DBMP_CHECK_LAUNCH("atlas_pack_kernel");
-  return DBMP_OK;
+  return launch_atlas_grid(tmpl, P, Ht, Wt, kind, out, st);
 }
 
 int launch_prepare(const Geom& g, const float* means2D, const float* radii, const float* rot, const float* opac,

@@ -91,6 +91,16 @@ int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
   g->kind = cv->atlas_kind;
   g->alpha_max = cv->alpha_max;
   g->t_stop = cv->t_stop;
+  if (cv->tile_size == 32) {
+    using L = Layout<32, DefaultNP<32>::v>;
+    g->fhx = 0.5f * (float)(L::FW - 1); g->fhy = 0.5f * (float)(L::FH - 1);
+  } else {
+    using L = Layout<16, DefaultNP<16>::v>;
+    g->fhx = 0.5f * (float)(L::FW - 1); g->fhy = 0.5f * (float)(L::FH - 1);
+  }
+  grid_shape(cv->tmpl_w, &g->gsx, &g->gGx);
+  grid_shape(cv->tmpl_h, &g->gsy, &g->gGy);
+  g->grid_off = (long long)atlas_grid_offset(g->P, g->Ht, g->Wt, g->kind);
   return DBMP_OK;
 }
 
@@ -220,7 +230,7 @@ int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas, 
   if (no_stop) g.t_stop = 0.f;
   REQUIRE(atlas && tile_offsets && tile_indices && counts, "dbmp_count: null pointer");
   REQUIRE(g.N == 0 || prim_info, "dbmp_count: prim_info is null");
-  cudaError_t e = cudaMemsetAsync(counts, 0, 7 * sizeof(unsigned long long), (cudaStream_t)stream);
+  cudaError_t e = cudaMemsetAsync(counts, 0, 10 * sizeof(unsigned long long), (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(counts)");
   return launch_count(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, counts,
                       (cudaStream_t)stream);

@@ -22,7 +22,9 @@ struct __align__(16) PrimInfo {
   float a00, a01, a10, a11;  // inverse affine to texel coordinates
   float alpha0, cr, cg, cb;  // alpha_max*sigmoid(opacity), sigmoid(colour logits)
   int toff;                  // first element of the template in the atlas; kNoFrag / kSolid
-  float rinv, cs, sn;        // reference r_inv and rotation cos/sin
+  int goff;                  // first cell of the template's clearance grid (packed atlases)
+  int gext;                  // clearance a warp footprint needs to be skipped (> kGridCap: never)
+  int pad;
 };
 static_assert(sizeof(PrimInfo) == 64, "PrimInfo must be 64 bytes");
 
@@ -49,6 +51,68 @@ __host__ __device__ inline int template_records(int kind, int Ht, int Wt) {
   return (kind == ATLAS_F16_PAIR || kind == ATLAS_BF16_PAIR) ? (Ht + 1) * Wt : Ht * Wt;
 }
 
+// Clearance grid of the packed atlas kinds.  Template texels are grouped in
+// cells of 2^gsx x 2^gsy; a cell stores the L-infinity distance, in texels and
+// capped at kGridCap, from its coordinate range to the nearest "support"
+// texel: value > kGridSupport or NaN.  The bilinear mask is a convex
+// combination of its four texels, so it can pass the fragment test
+// mask > 1e-6 (tile_forward.cu:271-276) only next to a support texel
+// (kGridSupport = 5e-7 leaves room for rounding and for half / bfloat16
+// storage).  A point whose clamped texel coordinate falls in a cell with
+// clearance D has no support texel within L-infinity distance < D, so a warp
+// footprint whose texel-space box (half extent e around the footprint centre)
+// satisfies e + 1 <= D yields no fragment.  The grid follows the texel
+// records, 256-byte aligned.
+constexpr int kGridCap = 64;
+constexpr float kGridSupport = 5e-7f;
+constexpr int kGridMaxCells = 64;   // cells per axis at most
+
+__host__ __device__ inline void grid_shape(int n, int* shift, int* cells) {
+  int s = 0;
+  while (((n + (1 << s) - 1) >> s) > kGridMaxCells) ++s;
+  *shift = s;
+  *cells = (n + (1 << s) - 1) >> s;
+}
+
+__host__ __device__ inline bool atlas_has_grid(int kind) { return kind != ATLAS_F32; }
+
+// Bytes of the texel records of an atlas kind (a packed atlas's grid follows them).
+__host__ __device__ inline size_t atlas_record_bytes(int P, int Ht, int Wt, int kind) {
+  const size_t recs = (size_t)P * template_records(kind, Ht, Wt);
+  switch (kind) {
+    case ATLAS_F32: return recs * 4;
+    case ATLAS_F32_QUAD: return recs * 16;
+    case ATLAS_F16_QUAD: case ATLAS_BF16_QUAD: return recs * 8;
+    case ATLAS_F16_PAIR: case ATLAS_BF16_PAIR: return recs * 4;
+    default: return 0;
+  }
+}
+__host__ __device__ inline size_t atlas_grid_offset(int P, int Ht, int Wt, int kind) {
+  return (atlas_record_bytes(P, Ht, Wt, kind) + 255) & ~(size_t)255;
+}
+
+// Thread layout of the tile walk: one CTA per TS x TS tile, NP pixels per
+// thread, each warp owning an FW x FH footprint.
+template <int TS, int NP>
+struct Layout {
+  static_assert(NP == 1 || NP == 2 || NP == 4, "pixels per thread");
+  static constexpr int FW = NP >= 2 ? 16 : 8;     // warp footprint
+  static constexpr int FH = NP == 4 ? 8 : 4;
+  static constexpr int WPR = TS / FW;              // warps per footprint row
+  static constexpr int NW = (TS / FW) * (TS / FH);
+  static constexpr int NT = NW * 32;
+  static __device__ __forceinline__ int ox(int p) { return 8 * (p & 1); }
+  static __device__ __forceinline__ int oy(int p) { return 4 * (p >> 1); }
+};
+
+// Pixels per thread of each tile size (tuned on B200).
+template <int TS> struct DefaultNP;
+#ifndef DBMP_NP32
+#define DBMP_NP32 2
+#endif
+template <> struct DefaultNP<32> { static constexpr int v = DBMP_NP32; };
+template <> struct DefaultNP<16> { static constexpr int v = 1; };
+
 struct Geom {
   int H, W, TS, tilesX, tilesY, T;
   int N, P, Ht, Wt;
@@ -58,6 +122,10 @@ struct Geom {
   float wm1, hm1;      // Wt-1, Ht-1
   float alpha_max;
   float t_stop;
+  float fhx, fhy;      // half extents (pixels) of the warp footprint of this tile size
+  int gsx, gsy;        // clearance grid: log2 of the cell size in texels
+  int gGx, gGy;        // clearance grid: cells per template row / column
+  long long grid_off;  // byte offset of the clearance grid in a packed atlas
 };
 
 // Bilinear neighbours (v00, v01, v10, v11) of texel (x0, y0); neighbours

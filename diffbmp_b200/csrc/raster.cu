@@ -14,19 +14,10 @@
 
 namespace dbmp {
 
-constexpr int kChunk = 32;   // list entries staged per barrier
-
-template <int TS, int NP>
-struct Layout {
-  static_assert(NP == 1 || NP == 2 || NP == 4, "pixels per thread");
-  static constexpr int FW = NP >= 2 ? 16 : 8;     // warp footprint
-  static constexpr int FH = NP == 4 ? 8 : 4;
-  static constexpr int WPR = TS / FW;              // warps per footprint row
-  static constexpr int NW = (TS / FW) * (TS / FH);
-  static constexpr int NT = NW * 32;
-  static __device__ __forceinline__ int ox(int p) { return 8 * (p & 1); }
-  static __device__ __forceinline__ int oy(int p) { return 4 * (p >> 1); }
-};
+#ifndef DBMP_CHUNK
+#define DBMP_CHUNK 32
+#endif
+constexpr int kChunk = DBMP_CHUNK;   // list entries staged per barrier
 
 // Stages entries [base, base+n) of the tile list: ids and PrimInfo records.
 template <int NT>
@@ -61,6 +52,22 @@ __device__ __forceinline__ bool footprint_miss(const float4& g0, float x0, float
 __device__ __forceinline__ bool footprint_inside(const float4& g0, float x0, float x1, float y0, float y1) {
   return (g0.x - g0.z <= x0 - 1.f) && (g0.x + g0.z >= x1 + 1.f) && (g0.y - g0.w <= y0 - 1.f) &&
          (g0.y + g0.w >= y1 + 1.f);
+}
+
+// Warp-uniform: true when the template's clearance grid shows that no pixel
+// of the warp footprint (centre (cx, cy)) can get a fragment from this
+// primitive.  The footprint centre's texel coordinate is clamped into the
+// template (clamping only shortens distances to its texels), and its cell's
+// clearance is compared with the primitive's requirement gext.
+__device__ __forceinline__ bool grid_clear(const Geom& g, const unsigned char* __restrict__ grid, const float4& g0,
+                                           const float4& g1, int goff, int gext, float cx, float cy) {
+  const float dx = cx - g0.x, dy = cy - g0.y;
+  const float tx = fminf(fmaxf(fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx)), 0.f), g.wm1);
+  const float ty = fminf(fmaxf(fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy)), 0.f), g.hm1);
+  float unused;
+  const int ix = floor_small(tx, &unused) >> g.gsx;
+  const int iy = floor_small(ty, &unused) >> g.gsy;
+  return (int)__ldg(grid + goff + iy * g.gGx + ix) >= gext;
 }
 
 // Texel coordinates, sampling position and fetched neighbours of one pixel.
@@ -129,11 +136,13 @@ struct TileWalker {
   static constexpr int NT = L::NT;
   static constexpr int NW = L::NW;
 
+  static constexpr bool kGrid = KIND != ATLAS_F32;   // packed atlases carry a clearance grid
+
   int warp, lane, start, end;
   float pxf[NP], pyf[NP];
   int px[NP], py[NP];
   bool valid[NP];
-  float fx0, fx1, fy0, fy1;
+  float fx0, fx1, fy0, fy1, fcx, fcy;
 
   __device__ __forceinline__ void init(const Geom& g, int tile, const int* __restrict__ offs) {
     warp = threadIdx.x >> 5;
@@ -155,17 +164,24 @@ struct TileWalker {
     fx1 = fx0 + (float)(L::FW - 1);
     fy0 = (float)(ty * TS + (warp / L::WPR) * L::FH);
     fy1 = fy0 + (float)(L::FH - 1);
+    fcx = fx0 + 0.5f * (float)(L::FW - 1);
+    fcy = fy0 + 0.5f * (float)(L::FH - 1);
   }
 
   // Forward walk.  STATS: counts (pixel, primitive) pairs that pass the cull
-  // and fragments composited, both before termination, plus walk statistics.
+  // and fragments composited, both before termination, plus walk statistics;
+  // it evaluates the clearance-grid test without skipping and counts the
+  // warp entries it would skip and, among them, those with a fragment (a
+  // correct grid gives 0).
   template <bool STATS = false>
   __device__ __forceinline__ void forward(const Geom& g, const PrimInfo* __restrict__ prims,
                                           const void* __restrict__ atlas, const int* __restrict__ idx,
                                           float4 (*s_pi)[4], int* s_id,
                                           float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP],
                                           unsigned long long* cnt = nullptr) {
-    unsigned long long n_cand = 0, n_frag = 0, n_went = 0, n_slots = 0, n_miss = 0;
+    unsigned long long n_cand = 0, n_frag = 0, n_went = 0, n_slots = 0, n_miss = 0, n_empty = 0, n_clear = 0,
+                       n_bad = 0;
+    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
     unsigned n_depth[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) n_depth[p] = 0;
@@ -190,13 +206,20 @@ struct TileWalker {
             if (STATS) ++n_miss;
             continue;
           }
-          const int toff = __float_as_int(s_pi[e][3].x);
+          const int4 q3 = *reinterpret_cast<const int4*>(&s_pi[e][3]);
+          const int toff = q3.x;
           if (toff == kNoFrag) continue;
           const float4 g1 = s_pi[e][1];
+          bool clear = false;
+          if (kGrid && toff != kSolid) {
+            clear = grid_clear(g, grid, g0, g1, q3.y, q3.z, fcx, fcy);
+            if (!STATS && clear) continue;
+          }
           const float4 g2 = s_pi[e][2];
           const int pos = base - start + e;
           if (STATS) {
             ++n_went;
+            n_clear += clear;
 #pragma unroll
             for (int p = 0; p < NP; ++p) n_slots += __popc(__ballot_sync(0xffffffffu, live[p]));
           }
@@ -228,6 +251,14 @@ struct TileWalker {
             }
           }
           bool local_done = true;
+          if (STATS) {
+            bool anyf = false;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) anyf = anyf || (s[p].ok && m[p] > 1e-6f);
+            anyf = __any_sync(0xffffffffu, anyf);
+            n_empty += !anyf;
+            n_bad += clear && anyf;
+          }
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
             const bool frag = s[p].ok && m[p] > 1e-6f;
@@ -262,6 +293,9 @@ struct TileWalker {
         atomicAdd(cnt + 4, n_slots);
         atomicAdd(cnt + 5, n_miss);
         atomicMax(cnt + 6, (unsigned long long)dmax);
+        atomicAdd(cnt + 7, n_empty);
+        atomicAdd(cnt + 8, n_clear);
+        atomicAdd(cnt + 9, n_bad);
       }
     }
   }
@@ -295,6 +329,7 @@ struct TileWalker {
       H[p] = 0.f;
       B[p] = 1.f;
     }
+    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
     for (int cb = (kmax / kChunk) * kChunk; cb >= 0; cb -= kChunk) {
       const int n = min(kChunk, end - start - cb);
       stage_chunk<NT>(prims, idx, g.N, start + cb, n, s_pi, s_id);
@@ -306,9 +341,11 @@ struct TileWalker {
         for (int k = 0; k < 8; ++k) acc[k] = 0.f;
         bool any = false;
         const float4 g0 = s_pi[e][0];
-        const int toff = __float_as_int(s_pi[e][3].x);
-        if (pos <= warp_max && toff != kNoFrag && !footprint_miss(g0, fx0, fx1, fy0, fy1)) {
-          const float4 g1 = s_pi[e][1];
+        const int4 q3 = *reinterpret_cast<const int4*>(&s_pi[e][3]);
+        const int toff = q3.x;
+        const float4 g1 = s_pi[e][1];
+        if (pos <= warp_max && toff != kNoFrag && !footprint_miss(g0, fx0, fx1, fy0, fy1) &&
+            !(kGrid && toff != kSolid && grid_clear(g, grid, g0, g1, q3.y, q3.z, fcx, fcy))) {
           const float4 g2 = s_pi[e][2];
           bool live[NP];
 #pragma unroll
@@ -411,20 +448,17 @@ struct TileWalker {
   }
 };
 
-// Pixels per thread of each tile size (tuned on B200).
-template <int TS> struct DefaultNP;
-#ifndef DBMP_NP32
-#define DBMP_NP32 2
-#endif
-template <> struct DefaultNP<32> { static constexpr int v = DBMP_NP32; };
-template <> struct DefaultNP<16> { static constexpr int v = 1; };
-
 template <int TS> constexpr int kThreadsOf() { return Layout<TS, DefaultNP<TS>::v>::NT; }
 // Resident CTAs per SM the register allocation is bounded for (walk kernels).
 #ifndef DBMP_MINBLOCKS256
 #define DBMP_MINBLOCKS256 3
 #endif
-template <int TS> constexpr int kBlocksPerSM() { return kThreadsOf<TS>() >= 512 ? 2 : DBMP_MINBLOCKS256; }
+#ifndef DBMP_MINBLOCKS512
+#define DBMP_MINBLOCKS512 2
+#endif
+template <int TS> constexpr int kBlocksPerSM() {
+  return kThreadsOf<TS>() >= 1024 ? 1 : kThreadsOf<TS>() >= 512 ? DBMP_MINBLOCKS512 : DBMP_MINBLOCKS256;
+}
 
 // ---------------------------------------------------------------------------
 template <int TS, int KIND>

@@ -81,8 +81,14 @@ int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* o
  *   t[y+1][x], t[y+1][x+1]; out holds P*Ht*Wt*4 elements;
  * *_PAIR: element (p,y,x) holds t[y][x], t[y][x+1] for y < Ht plus one zero
  *   row y = Ht; out holds P*(Ht+1)*Wt*2 elements.
- * Neighbours outside the template are 0.  dbmp_atlas_bytes gives the size.
- * No reference counterpart (storage format of the precision form). */
+ * Neighbours outside the template are 0.  The texel records are followed,
+ * at the next 256-byte boundary, by a clearance grid: per template, cells of
+ * 2^s x 2^t texels (s, t the smallest shifts giving at most 64 cells per
+ * axis), one byte each, the L-infinity distance in texels (capped at 64) from
+ * the cell to the nearest texel > 5e-7 or NaN.  The tile walk uses it to skip
+ * warp footprints where a primitive's mask cannot pass the fragment test
+ * mask > 1e-6.  dbmp_atlas_bytes gives the total size.  No reference
+ * counterpart (storage format of the precision form). */
 size_t dbmp_atlas_bytes(int P, int Ht, int Wt, int kind);
 int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, void* out, void* stream);
 
@@ -178,10 +184,13 @@ int dbmp_backward_noalloc_max_prims(void);
  * entries (sum over tiles), counts[3] = (warp, entry) pairs a warp evaluated,
  * counts[4] = pixel slots still running summed over those pairs, counts[5] =
  * (warp, entry) pairs rejected by the warp-footprint test, counts[6] = the
- * largest number of fragments composited at one pixel.  cv->t_stop may be 0
- * here to count without termination (every fragment, as the reference
- * composites).  counts: 7 device u64, zeroed by the call.  Used for roofline
- * and memory accounting; no reference counterpart. */
+ * largest number of fragments composited at one pixel, counts[7] = walked
+ * (warp, entry) pairs without any fragment, counts[8] = walked pairs the
+ * packed atlas's clearance grid skips, counts[9] = pairs the grid would skip
+ * although they hold a fragment (0 unless the grid is wrong).  cv->t_stop may
+ * be 0 here to count without termination (every fragment, as the reference
+ * composites).  counts: 10 device u64, zeroed by the call.  Used for roofline
+ * and memory accounting and to check the grid; no reference counterpart. */
 int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
                const int32_t* tile_offsets, const int32_t* tile_indices,
                unsigned long long* counts, void* stream);

@@ -39,7 +39,7 @@ def test_memory_4096_n100k():
     # deepest pixel without termination, i.e. the cache depth the reference would need
     cv = rz.canvas(N, atlas)
     cv.t_stop = 0.0
-    cnt = torch.zeros(7, dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(10, dtype=torch.int64, device="cuda")
     call("dbmp_count", ctypes.byref(cv), _ptr(state.prim_info), _ptr(atlas.data), _ptr(state.lists.offsets),
          _ptr(state.lists.indices), _ptr(cnt), _stream())
     K = int(cnt[6].item())

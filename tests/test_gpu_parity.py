@@ -129,22 +129,25 @@ def _spec_scene(cfg, seed, **over):
                    s.alpha_max)
 
 
+@pytest.mark.parametrize("kind", ["f32", "f32q"])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_forward_parity_gpu(name):
+def test_forward_parity_gpu(name, kind):
+    """f32: reference atlas layout; f32q: packed quads with the clearance-grid skip."""
     sc = SCENES[name]()
     offs, idx = bin_scene(sc)
-    color, alpha, state, *_ = ours_forward(sc)
+    color, alpha, state, *_ = ours_forward(sc, kind=kind)
     r = check_image(sc, offs, idx, color, alpha)
     # per-pixel last contributor never exceeds the oracle's fragment list
     assert state.last_pos.max().item() < max(len(idx), 1)
     print(name, r["max_err"], r["sensitive"])
 
 
+@pytest.mark.parametrize("kind", ["f32", "f32q"])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_backward_parity_gpu(name):
+def test_backward_parity_gpu(name, kind):
     sc = SCENES[name]()
     offs, idx = bin_scene(sc)
-    color, alpha, state, rz, atlas, d = ours_forward(sc)
+    color, alpha, state, rz, atlas, d = ours_forward(sc, kind=kind)
     rng = np.random.default_rng(7)
     gc = rng.normal(0, 1, (sc.H, sc.W, 3)).astype(np.float32)
     ga = rng.normal(0, 1, (sc.H, sc.W)).astype(np.float32)
@@ -208,3 +211,79 @@ def test_precision_forms_gpu(kind, min_psnr):
     psnr = 10 * np.log10(1.0 / max(mse, 1e-30))
     print(kind, "PSNR", psnr, "max", np.abs(color - ref["color"]).max())
     assert psnr >= min_psnr
+
+
+# ---------------------------------------------------------------------------
+# clearance grid of the packed atlases
+def _grid_bruteforce(t, cap=64, max_cells=64):
+    """Per cell: min over support texels (> 5e-7 or NaN) of the L-infinity
+    distance from the cell's coordinate range to the texel, capped (the
+    definition, evaluated directly)."""
+    Ht, Wt = t.shape
+
+    def shape(n):
+        s = 0
+        while -(-n // (1 << s)) > max_cells:
+            s += 1
+        return s, -(-n // (1 << s))
+    sx, gx = shape(Wt)
+    sy, gy = shape(Ht)
+    ys, xs = np.nonzero(~(t <= 5e-7))
+    out = np.full((gy, gx), cap, np.int64)
+    for iy in range(gy):
+        ylo, yhi = iy << sy, min((iy + 1) << sy, Ht - 1)
+        dy = np.maximum(0, np.maximum(ylo - ys, ys - yhi))
+        for ix in range(gx):
+            xlo, xhi = ix << sx, min((ix + 1) << sx, Wt - 1)
+            dx = np.maximum(0, np.maximum(xlo - xs, xs - xhi))
+            if len(xs):
+                out[iy, ix] = min(cap, int(np.maximum(dx, dy).min()))
+    return out
+
+
+@pytest.mark.parametrize("kind,rec_bytes,extra_row", [("f32q", 16, 0), ("f16", 4, 1), ("bf16q", 8, 0)])
+@pytest.mark.parametrize("Ht,Wt", [(40, 72), (130, 130), (300, 20)])
+def test_clearance_grid_matches_definition_gpu(kind, rec_bytes, extra_row, Ht, Wt):
+    from diffbmp_b200 import workloads as wl
+    rng = np.random.default_rng(Ht * 7 + Wt)
+    P = 3
+    T = np.zeros((P, Ht, Wt), np.float32)
+    for p in range(P):
+        sh = wl.random_shape(rng, max(Ht, Wt))[:Ht, :Wt]
+        T[p] = np.where(sh > 0.5, sh, 0.0)          # hard zero outside the shape
+    T[2, Ht // 3, Wt // 2] = np.nan                   # NaN texels count as support
+    T[2, 1, 1] = -0.5                                 # negative texels do not
+    T[1, 2, Wt - 3] = 4e-7                            # nor texels at or below 5e-7
+    T[0, Ht - 2, 3] = 6e-7                            # above it they do
+    atlas = R.Atlas(torch.from_numpy(T).cuda(), kind)
+    raw = atlas.data.cpu().numpy()
+    off = (P * (Ht + extra_row) * Wt * rec_bytes + 255) // 256 * 256
+    for p in range(P):
+        want = _grid_bruteforce(T[p])
+        n = want.size
+        got = raw[off + p * n: off + (p + 1) * n].reshape(want.shape).astype(np.int64)
+        assert np.array_equal(got, want), (p, np.argwhere(got != want)[:5])
+    assert raw.size == off + P * want.size
+
+
+@pytest.mark.parametrize("kind", ["f32q", "f16", "bf16"])
+@pytest.mark.parametrize("name", list(SCENES))
+@pytest.mark.parametrize("t_stop", [1e-6, 0.0])
+def test_clearance_grid_never_skips_a_fragment_gpu(name, kind, t_stop):
+    """The counting walk evaluates the grid test on every walked warp entry:
+    none that the grid skips may hold a fragment."""
+    import ctypes
+    from diffbmp_b200._lib import call
+    sc = SCENES[name]()
+    color, alpha, state, rz, atlas, d = ours_forward(sc, kind=kind)
+    cv = rz.canvas(sc.N, atlas)
+    cv.t_stop = t_stop
+    cnt = torch.zeros(10, dtype=torch.int64, device="cuda")
+    call("dbmp_count", ctypes.byref(cv), R._ptr(state.prim_info), R._ptr(atlas.data), R._ptr(state.lists.offsets),
+         R._ptr(state.lists.indices), R._ptr(cnt), R._stream())
+    c = cnt.tolist()
+    print(name, kind, t_stop, "walked", c[3], "empty", c[7], "grid skips", c[8], "bad", c[9])
+    assert c[9] == 0
+    assert c[8] <= c[7]
+    if name == "atlas128":        # random shapes leave empty cells (the c0 soft disk has none)
+        assert c[8] > 0
