@@ -3,40 +3,26 @@
 // One CTA owns one tile of TS x TS pixels; each thread owns NP pixels
 // (NP = 4, 2 or 1) of a compact warp footprint (16x8, 16x4 or 8x4 pixels) so
 // that a primitive's square cull is mostly warp-uniform and the warp's texel
-// fetches stay close together in the atlas.  The tile's primitive list is
-// walked in chunks of kChunk entries whose 64-byte PrimInfo records are staged
-// in shared memory once per CTA.  Per entry a thread first computes the texel
-// coordinates of all its pixels and issues all their texel loads (addresses
-// of pixels without a fragment are redirected to texel 0 of the template, so
-// every load is in bounds), then composites them branch-free; warps whose
-// pixels are all below t_stop skip the math but keep joining the barriers.
+// fetches stay close together in the atlas.
+//
+// Every warp walks the tile's primitive list on its own, without CTA
+// barriers: it stages 32 list entries at a time into a warp-private shared
+// buffer (lane i loads entry i's 64-byte PrimInfo record and runs the
+// warp-footprint cull and the clearance-grid test for it), and a ballot of
+// the survivors gives the entries the warp composites, in list order in the
+// forward walk and in reverse order in the backward walk.  Per entry a thread
+// first computes the texel coordinates of all its pixels and issues their
+// texel loads (addresses of pixels without a fragment are redirected to texel
+// 0 of the template, so every load is in bounds), then composites them
+// branch-free.  A warp stops when all its pixels are below t_stop; the
+// backward walk of a warp starts at its own last contributor and adds its
+// warp-reduced per-primitive sums straight into the FP64 accumulator.
 #include "dbmp_internal.cuh"
 
 namespace dbmp {
 
-#ifndef DBMP_CHUNK
-#define DBMP_CHUNK 32
-#endif
-constexpr int kChunk = DBMP_CHUNK;   // list entries staged per barrier
-
-// Stages entries [base, base+n) of the tile list: ids and PrimInfo records.
-template <int NT>
-__device__ __forceinline__ void stage_chunk(const PrimInfo* __restrict__ prims, const int* __restrict__ idx,
-                                            int N, int base, int n, float4 (*s_pi)[4], int* s_id) {
-  for (int i = threadIdx.x; i < 4 * n; i += NT) {
-    const int e = i >> 2, q = i & 3;
-    const int id = __ldg(idx + base + e);
-    float4 v;
-    if (id >= 0 && id < N) {
-      v = __ldg(reinterpret_cast<const float4*>(prims + id) + q);
-    } else {  // out-of-range ids are skipped like tile_forward.cu:184-185
-      v = make_float4(0.f, 0.f, -1.f, -1.f);
-      if (q == 3) v.x = __int_as_float(kNoFrag);
-    }
-    s_pi[e][q] = v;
-    if (q == 0) s_id[e] = (id >= 0 && id < N) ? id : -1;
-  }
-}
+constexpr int kChunk = 32;   // list entries staged per warp at a time (one per lane)
+constexpr unsigned kFull = 0xffffffffu;
 
 // Conservative warp-uniform rejection: true when the primitive's cull square
 // misses every pixel of the warp footprint (1 px margin for rounding; NaN
@@ -130,17 +116,23 @@ __device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
 }
 
 // ---------------------------------------------------------------------------
+// Ballots of one staged chunk (bit j = entry base + j).
+struct ChunkMasks {
+  unsigned todo;     // entries the warp composites
+  unsigned inside;   // footprint entirely inside the entry's cull square
+  unsigned clear;    // clearance grid shows no fragment (skipped unless counting)
+  unsigned miss;     // footprint misses the cull square
+};
+
 template <int TS, int NP, int KIND>
 struct TileWalker {
   using L = Layout<TS, NP>;
   static constexpr int NT = L::NT;
   static constexpr int NW = L::NW;
-
   static constexpr bool kGrid = KIND != ATLAS_F32;   // packed atlases carry a clearance grid
 
   int warp, lane, start, end;
   float pxf[NP], pyf[NP];
-  int px[NP], py[NP];
   bool valid[NP];
   float fx0, fx1, fy0, fy1, fcx, fcy;
 
@@ -150,15 +142,12 @@ struct TileWalker {
     const int tx = tile % g.tilesX, ty = tile / g.tilesX;
     start = __ldg(offs + tile);
     end = __ldg(offs + tile + 1);
-    const int bx = tx * TS + (warp % L::WPR) * L::FW + (lane & 7);
-    const int by = ty * TS + (warp / L::WPR) * L::FH + (lane >> 3);
+    const int bx = px(tile, g, 0), by = py(tile, g, 0);
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      px[p] = bx + L::ox(p);
-      py[p] = by + L::oy(p);
-      pxf[p] = (float)px[p];
-      pyf[p] = (float)py[p];
-      valid[p] = px[p] < g.W && py[p] < g.H;
+      pxf[p] = (float)(bx + L::ox(p));
+      pyf[p] = (float)(by + L::oy(p));
+      valid[p] = bx + L::ox(p) < g.W && by + L::oy(p) < g.H;
     }
     fx0 = (float)(tx * TS + (warp % L::WPR) * L::FW);
     fx1 = fx0 + (float)(L::FW - 1);
@@ -166,6 +155,64 @@ struct TileWalker {
     fy1 = fy0 + (float)(L::FH - 1);
     fcx = fx0 + 0.5f * (float)(L::FW - 1);
     fcy = fy0 + 0.5f * (float)(L::FH - 1);
+  }
+
+  // Pixel coordinates of pixel p of this thread.
+  __device__ __forceinline__ int px(int tile, const Geom& g, int p) const {
+    return (tile % g.tilesX) * TS + (warp % L::WPR) * L::FW + (lane & 7) + L::ox(p);
+  }
+  __device__ __forceinline__ int py(int tile, const Geom& g, int p) const {
+    return (tile / g.tilesX) * TS + (warp / L::WPR) * L::FH + (lane >> 3) + L::oy(p);
+  }
+
+  // Stages list positions [base, min(base + 32, stop)) into the warp's buffer
+  // w (lane i: position base + i) and returns the chunk's ballots.  With
+  // KEEP_CLEAR, entries the clearance grid rules out stay in `todo` (the
+  // counting walk checks them).  Out-of-range primitive ids never yield a
+  // fragment (tile_forward.cu:184-185).  my_id: this lane's primitive id.
+  template <bool KEEP_CLEAR>
+  __device__ __forceinline__ ChunkMasks stage(const Geom& g, const PrimInfo* __restrict__ prims,
+                                              const int* __restrict__ idx, const unsigned char* __restrict__ grid,
+                                              int base, int stop, float4 (*w)[4], int* my_id) {
+    bool keep = false, inside = false, clear = false, miss = false;
+    int id = -1;
+    __syncwarp();   // every lane is done with the previous chunk's records
+    const int pos = base + lane;
+    if (pos < stop) {
+      id = __ldg(idx + pos);
+      if (id >= 0 && id < g.N) {
+        const float4* r = reinterpret_cast<const float4*>(prims + id);
+        const float4 g0 = __ldg(r);
+        miss = footprint_miss(g0, fx0, fx1, fy0, fy1);
+        if (!miss) {
+          const float4 q = __ldg(r + 3);
+          const int toff = __float_as_int(q.x);
+          if (toff != kNoFrag) {
+            const float4 g1 = __ldg(r + 1);
+            if (kGrid && toff != kSolid)
+              clear = grid_clear(g, grid, g0, g1, __float_as_int(q.y), __float_as_int(q.z), fcx, fcy);
+            keep = KEEP_CLEAR || !clear;
+            if (keep) {
+              inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
+              w[lane][0] = g0;
+              w[lane][1] = g1;
+              w[lane][2] = __ldg(r + 2);
+              w[lane][3] = q;
+            }
+          }
+        }
+      } else {
+        id = -1;
+      }
+    }
+    __syncwarp();   // the records are visible to every lane
+    *my_id = id;
+    ChunkMasks m;
+    m.todo = __ballot_sync(kFull, keep);
+    m.inside = __ballot_sync(kFull, inside);
+    m.clear = KEEP_CLEAR ? __ballot_sync(kFull, clear) : 0u;
+    m.miss = KEEP_CLEAR ? __ballot_sync(kFull, miss) : 0u;
+    return m;
   }
 
   // Forward walk.  STATS: counts (pixel, primitive) pairs that pass the cull
@@ -176,15 +223,13 @@ struct TileWalker {
   template <bool STATS = false>
   __device__ __forceinline__ void forward(const Geom& g, const PrimInfo* __restrict__ prims,
                                           const void* __restrict__ atlas, const int* __restrict__ idx,
-                                          float4 (*s_pi)[4], int* s_id,
+                                          float4 (*w)[4],
                                           float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP],
                                           unsigned long long* cnt = nullptr) {
     unsigned long long n_cand = 0, n_frag = 0, n_went = 0, n_slots = 0, n_miss = 0, n_empty = 0, n_clear = 0,
                        n_bad = 0;
-    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
     unsigned n_depth[NP];
-#pragma unroll
-    for (int p = 0; p < NP; ++p) n_depth[p] = 0;
+    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
     bool live[NP];
     bool all_done = true;
 #pragma unroll
@@ -192,94 +237,85 @@ struct TileWalker {
       C[p][0] = C[p][1] = C[p][2] = 0.f;
       T[p] = 1.f; Tl[p] = 1.f; lp[p] = -1;
       live[p] = valid[p];
+      n_depth[p] = 0;
       all_done = all_done && !live[p];
     }
-    bool warp_done = __all_sync(0xffffffffu, all_done);
-    for (int base = start; base < end; base += kChunk) {
-      const int n = min(kChunk, end - base);
-      stage_chunk<NT>(prims, idx, g.N, base, n, s_pi, s_id);
-      __syncthreads();
-      if (!warp_done) {
-        for (int e = 0; e < n; ++e) {
-          const float4 g0 = s_pi[e][0];
-          if (footprint_miss(g0, fx0, fx1, fy0, fy1)) {
-            if (STATS) ++n_miss;
-            continue;
-          }
-          const int4 q3 = *reinterpret_cast<const int4*>(&s_pi[e][3]);
-          const int toff = q3.x;
-          if (toff == kNoFrag) continue;
-          const float4 g1 = s_pi[e][1];
-          bool clear = false;
-          if (kGrid && toff != kSolid) {
-            clear = grid_clear(g, grid, g0, g1, q3.y, q3.z, fcx, fcy);
-            if (!STATS && clear) continue;
-          }
-          const float4 g2 = s_pi[e][2];
-          const int pos = base - start + e;
-          if (STATS) {
-            ++n_went;
-            n_clear += clear;
+    bool warp_done = __all_sync(kFull, all_done);
+    for (int base = start; base < end && !warp_done; base += kChunk) {
+      int my_id;
+      const ChunkMasks cm = stage<STATS>(g, prims, idx, grid, base, end, w, &my_id);
+      unsigned todo = cm.todo;
+      if (STATS) n_miss += __popc(cm.miss);
+      while (todo) {
+        const int e = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const float4 g0 = w[e][0];
+        const float4 g1 = w[e][1];
+        const float4 g2 = w[e][2];
+        const int toff = __float_as_int(w[e][3].x);
+        const int pos = base - start + e;
+        const bool clear = (cm.clear >> e) & 1u;
+        if (STATS) {
+          ++n_went;
+          n_clear += clear;
 #pragma unroll
-            for (int p = 0; p < NP; ++p) n_slots += __popc(__ballot_sync(0xffffffffu, live[p]));
-          }
-          Sample s[NP];
-          float m[NP];
-          if (toff != kSolid) {
-            entry_coords<NP, L>(g, g0, g1, footprint_inside(g0, fx0, fx1, fy0, fy1), pxf, pyf, live, s);
-            bool any[NP];
+          for (int p = 0; p < NP; ++p) n_slots += __popc(__ballot_sync(kFull, live[p]));
+        }
+        Sample s[NP];
+        float m[NP];
+        if (toff != kSolid) {
+          entry_coords<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, pxf, pyf, live, s);
+          bool any[NP];
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              any[p] = __any_sync(0xffffffffu, s[p].ok);
-              if (any[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
-            }
-#pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              m[p] = any[p] ? blend<false>(s[p], nullptr, nullptr) : 0.f;
-              if (STATS) {
-                const bool c = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
-                n_cand += c;
-              }
-            }
-          } else {
-            // NaN geometry: every live pixel that passes the cull gets mask 1
-#pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              s[p].ok = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
-              m[p] = 1.f;
-              if (STATS) n_cand += s[p].ok;
-            }
-          }
-          bool local_done = true;
-          if (STATS) {
-            bool anyf = false;
-#pragma unroll
-            for (int p = 0; p < NP; ++p) anyf = anyf || (s[p].ok && m[p] > 1e-6f);
-            anyf = __any_sync(0xffffffffu, anyf);
-            n_empty += !anyf;
-            n_bad += clear && anyf;
+          for (int p = 0; p < NP; ++p) {
+            any[p] = __any_sync(kFull, s[p].ok);
+            if (any[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
           }
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
-            const bool frag = s[p].ok && m[p] > 1e-6f;
-            if (STATS) { n_frag += frag; n_depth[p] += frag; }
-            if (__any_sync(0xffffffffu, frag)) {
-              const float a = frag ? g2.x * m[p] : 0.f;
-              const float w = T[p] * a;
-              C[p][0] = fmaf(w, g2.y, C[p][0]);
-              C[p][1] = fmaf(w, g2.z, C[p][1]);
-              C[p][2] = fmaf(w, g2.w, C[p][2]);
-              Tl[p] = frag ? T[p] : Tl[p];
-              lp[p] = frag ? pos : lp[p];
-              T[p] *= fmaxf(1.f - a, 0.f);
-              live[p] = live[p] && !(T[p] < g.t_stop);
+            m[p] = any[p] ? blend<false>(s[p], nullptr, nullptr) : 0.f;
+            if (STATS) {
+              const bool c = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+              n_cand += c;
             }
-            local_done = local_done && !live[p];
           }
-          if (__all_sync(0xffffffffu, local_done)) { warp_done = true; break; }
+        } else {
+          // NaN geometry: every live pixel that passes the cull gets mask 1
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            s[p].ok = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+            m[p] = 1.f;
+            if (STATS) n_cand += s[p].ok;
+          }
         }
+        if (STATS) {
+          bool anyf = false;
+#pragma unroll
+          for (int p = 0; p < NP; ++p) anyf = anyf || (s[p].ok && m[p] > 1e-6f);
+          anyf = __any_sync(kFull, anyf);
+          n_empty += !anyf;
+          n_bad += clear && anyf;
+        }
+        bool local_done = true;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const bool frag = s[p].ok && m[p] > 1e-6f;
+          if (STATS) { n_frag += frag; n_depth[p] += frag; }
+          if (__any_sync(kFull, frag)) {
+            const float a = frag ? g2.x * m[p] : 0.f;
+            const float wt = T[p] * a;
+            C[p][0] = fmaf(wt, g2.y, C[p][0]);
+            C[p][1] = fmaf(wt, g2.z, C[p][1]);
+            C[p][2] = fmaf(wt, g2.w, C[p][2]);
+            Tl[p] = frag ? T[p] : Tl[p];
+            lp[p] = frag ? pos : lp[p];
+            T[p] *= fmaxf(1.f - a, 0.f);
+            live[p] = live[p] && !(T[p] < g.t_stop);
+          }
+          local_done = local_done && !live[p];
+        }
+        if (__all_sync(kFull, local_done)) { warp_done = true; break; }
       }
-      if (__syncthreads_and(warp_done)) break;
     }
     if (STATS) {
       atomicAdd(cnt + 0, n_cand);
@@ -287,7 +323,7 @@ struct TileWalker {
       unsigned dmax = 0;
 #pragma unroll
       for (int p = 0; p < NP; ++p) dmax = max(dmax, n_depth[p]);
-      dmax = __reduce_max_sync(0xffffffffu, dmax);
+      dmax = __reduce_max_sync(kFull, dmax);
       if (lane == 0) {
         atomicAdd(cnt + 3, n_went);
         atomicAdd(cnt + 4, n_slots);
@@ -301,24 +337,21 @@ struct TileWalker {
   }
 
   // Reverse walk.  gC/gA: upstream gradients per pixel; Ts: on entry the T
-  // entering each pixel's last contributor (lp).  Per-primitive partial sums
-  // are reduced in the warp, then across the CTA, and accumulated into gacc
-  // (N,8) f64 (layout documented at finalize_kernel).
+  // entering each pixel's last contributor (lp).  Per entry the warp reduces
+  // its per-primitive partial sums and lanes 0..7 add them to gacc (N,8) f64
+  // (layout documented at finalize_kernel).
   __device__ __forceinline__ void backward(const Geom& g, const PrimInfo* __restrict__ prims,
                                            const void* __restrict__ atlas, const int* __restrict__ idx,
-                                           float4 (*s_pi)[4], int* s_id, float (*s_part)[kChunk][8],
-                                           int* s_kmax, const float (&gC)[NP][3], const float (&gA)[NP],
+                                           float4 (*w)[4], const float (&gC)[NP][3], const float (&gA)[NP],
                                            float (&Ts)[NP], const int (&lp)[NP], double* __restrict__ gacc) {
     int my_max = -1;
 #pragma unroll
     for (int p = 0; p < NP; ++p) my_max = max(my_max, lp[p]);
-    const int warp_max = __reduce_max_sync(0xffffffffu, my_max);
-    if (threadIdx.x == 0) *s_kmax = -1;
-    __syncthreads();
-    if (lane == 0) atomicMax(s_kmax, warp_max);
-    __syncthreads();
-    const int kmax = *s_kmax;
-    if (kmax < 0) return;
+    const int warp_max = __reduce_max_sync(kFull, my_max);
+    if (warp_max < 0) return;
+    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
+    // sum index that lane l < 8 holds after the recursive-halving reduction
+    const int kidx = 4 * (lane & 1) + 2 * ((lane >> 1) & 1) + ((lane >> 2) & 1);
 
     // H = gC . R and B = prod(1 - a) over the fragments behind the current
     // one, where R is their colour composited from T = 1; both obey
@@ -329,121 +362,107 @@ struct TileWalker {
       H[p] = 0.f;
       B[p] = 1.f;
     }
-    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
-    for (int cb = (kmax / kChunk) * kChunk; cb >= 0; cb -= kChunk) {
-      const int n = min(kChunk, end - start - cb);
-      stage_chunk<NT>(prims, idx, g.N, start + cb, n, s_pi, s_id);
-      __syncthreads();
-      for (int e = n - 1; e >= 0; --e) {
+    for (int cb = (warp_max / kChunk) * kChunk; cb >= 0; cb -= kChunk) {
+      int my_id;
+      const ChunkMasks cm = stage<false>(g, prims, idx, grid, start + cb, start + warp_max + 1, w, &my_id);
+      unsigned todo = cm.todo;
+      while (todo) {
+        const int e = 31 - __clz(todo);
+        todo &= ~(1u << e);
         const int pos = cb + e;
+        const int id = __shfl_sync(kFull, my_id, e);
+        const float4 g0 = w[e][0];
+        const float4 g1 = w[e][1];
+        const float4 g2 = w[e][2];
+        const int toff = __float_as_int(w[e][3].x);
         float acc[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) acc[k] = 0.f;
         bool any = false;
-        const float4 g0 = s_pi[e][0];
-        const int4 q3 = *reinterpret_cast<const int4*>(&s_pi[e][3]);
-        const int toff = q3.x;
-        const float4 g1 = s_pi[e][1];
-        if (pos <= warp_max && toff != kNoFrag && !footprint_miss(g0, fx0, fx1, fy0, fy1) &&
-            !(kGrid && toff != kSolid && grid_clear(g, grid, g0, g1, q3.y, q3.z, fcx, fcy))) {
-          const float4 g2 = s_pi[e][2];
-          bool live[NP];
+        bool live[NP];
 #pragma unroll
-          for (int p = 0; p < NP; ++p) live[p] = pos <= lp[p];
-          Sample s[NP];
-          float m[NP], gx[NP], gy[NP];
-          bool anyp[NP];
-          if (toff != kSolid) {
-            entry_coords<NP, L>(g, g0, g1, footprint_inside(g0, fx0, fx1, fy0, fy1), pxf, pyf, live, s);
+        for (int p = 0; p < NP; ++p) live[p] = pos <= lp[p];
+        Sample s[NP];
+        float m[NP], gx[NP], gy[NP];
+        bool anyp[NP];
+        if (toff != kSolid) {
+          entry_coords<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, pxf, pyf, live, s);
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              anyp[p] = __any_sync(0xffffffffu, s[p].ok);
-              if (anyp[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
-            }
-#pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              m[p] = 0.f; gx[p] = gy[p] = 0.f;
-              if (anyp[p]) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
-            }
-          } else {
-#pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              const float dx = pxf[p] - g0.x, dy = pyf[p] - g0.y;
-              s[p].ok = live[p] && !(fabsf(dx) > g0.z || fabsf(dy) > g0.w);
-              s[p].tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
-              s[p].ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
-              m[p] = 1.f;
-              gx[p] = gy[p] = __int_as_float(0x7fc00000);
-            }
+          for (int p = 0; p < NP; ++p) {
+            anyp[p] = __any_sync(kFull, s[p].ok);
+            if (anyp[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
           }
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
-            const bool frag = s[p].ok && m[p] > 1e-6f;
-            if (!__any_sync(0xffffffffu, frag)) continue;
-            const float a = frag ? g2.x * m[p] : 0.f;
-            const float om = fmaxf(1.f - a, 0.f);
-            // T entering this fragment: stored for the last contributor, else
-            // undo the forward product (om >= t_stop > 0 for every earlier
-            // fragment, so the fast division is well conditioned; om = 1 and
-            // Ts is unchanged when there is no fragment).
-            const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
-            Ts[p] = Tk;
-            const float gCc = fmaf(gC[p][0], g2.y, fmaf(gC[p][1], g2.z, gC[p][2] * g2.w));
-            const float dLda = frag ? Tk * (gCc - H[p] + gA[p] * B[p]) : 0.f;
-            const float u = dLda * gx[p], v = dLda * gy[p];
-            const float ex = s[p].tx - g.hx, ey = s[p].ty - g.hy;
-            acc[0] += u;
-            acc[1] += v;
-            acc[2] = fmaf(u, ex, fmaf(v, ey, acc[2]));
-            acc[3] = fmaf(u * g.rxy, ey, fmaf(-v * g.ryx, ex, acc[3]));
-            const float w = a * Tk;
-            acc[4] = fmaf(gC[p][0], w, acc[4]);
-            acc[5] = fmaf(gC[p][1], w, acc[5]);
-            acc[6] = fmaf(gC[p][2], w, acc[6]);
-            acc[7] = fmaf(dLda, a, acc[7]);
-            H[p] = fmaf(om, H[p], a * gCc);
-            B[p] *= om;
-            any = any || frag;
+            m[p] = 0.f; gx[p] = gy[p] = 0.f;
+            if (anyp[p]) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
+          }
+        } else {
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            const float dx = pxf[p] - g0.x, dy = pyf[p] - g0.y;
+            s[p].ok = live[p] && !(fabsf(dx) > g0.z || fabsf(dy) > g0.w);
+            s[p].tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
+            s[p].ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
+            m[p] = 1.f;
+            gx[p] = gy[p] = __int_as_float(0x7fc00000);
           }
         }
-        if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const bool frag = s[p].ok && m[p] > 1e-6f;
+          if (!__any_sync(kFull, frag)) continue;
+          const float a = frag ? g2.x * m[p] : 0.f;
+          const float om = fmaxf(1.f - a, 0.f);
+          // T entering this fragment: stored for the last contributor, else
+          // undo the forward product (om >= t_stop > 0 for every earlier
+          // fragment, so the fast division is well conditioned; om = 1 and
+          // Ts is unchanged when there is no fragment).
+          const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
+          Ts[p] = Tk;
+          const float gCc = fmaf(gC[p][0], g2.y, fmaf(gC[p][1], g2.z, gC[p][2] * g2.w));
+          const float dLda = frag ? Tk * (gCc - H[p] + gA[p] * B[p]) : 0.f;
+          const float u = dLda * gx[p], v = dLda * gy[p];
+          const float ex = s[p].tx - g.hx, ey = s[p].ty - g.hy;
+          acc[0] += u;
+          acc[1] += v;
+          acc[2] = fmaf(u, ex, fmaf(v, ey, acc[2]));
+          acc[3] = fmaf(u * g.rxy, ey, fmaf(-v * g.ryx, ex, acc[3]));
+          const float wt = a * Tk;
+          acc[4] = fmaf(gC[p][0], wt, acc[4]);
+          acc[5] = fmaf(gC[p][1], wt, acc[5]);
+          acc[6] = fmaf(gC[p][2], wt, acc[6]);
+          acc[7] = fmaf(dLda, a, acc[7]);
+          H[p] = fmaf(om, H[p], a * gCc);
+          B[p] *= om;
+          any = any || frag;
+        }
+        if (__any_sync(kFull, any)) {
           // recursive-halving reduction: 8 sums over 32 lanes in 9 shuffles;
-          // lane l (l < 8) ends with sum index 4*(l&1) + 2*((l>>1)&1) + ((l>>2)&1)
+          // lane l (l < 8) ends with sum index kidx
           const bool b0 = lane & 1, b1 = lane & 2, b2 = lane & 4;
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             const float send = b0 ? acc[k] : acc[k + 4];
             const float keep = b0 ? acc[k + 4] : acc[k];
-            acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+            acc[k] = keep + __shfl_xor_sync(kFull, send, 1);
           }
 #pragma unroll
           for (int k = 0; k < 2; ++k) {
             const float send = b1 ? acc[k] : acc[k + 2];
             const float keep = b1 ? acc[k + 2] : acc[k];
-            acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+            acc[k] = keep + __shfl_xor_sync(kFull, send, 2);
           }
           {
             const float send = b2 ? acc[0] : acc[1];
             const float keep = b2 ? acc[1] : acc[0];
-            acc[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+            acc[0] = keep + __shfl_xor_sync(kFull, send, 4);
           }
-          acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 8);
-          acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 16);
-          if (lane < 8) s_part[warp][e][4 * (lane & 1) + 2 * ((lane >> 1) & 1) + ((lane >> 2) & 1)] = acc[0];
-        } else if (lane < 8) {
-          s_part[warp][e][lane] = 0.f;
+          acc[0] += __shfl_xor_sync(kFull, acc[0], 8);
+          acc[0] += __shfl_xor_sync(kFull, acc[0], 16);
+          if (lane < 8 && acc[0] != 0.f) atomicAdd(gacc + (size_t)id * 8 + kidx, (double)acc[0]);
         }
       }
-      __syncthreads();
-      // CTA reduction over the warps; one f64 atomic per non-zero sum.
-      for (int i = threadIdx.x; i < n * 8; i += NT) {
-        const int e = i >> 3, k = i & 7;
-        float s = 0.f;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) s += s_part[w][e][k];
-        if (s != 0.f && s_id[e] >= 0) atomicAdd(gacc + (size_t)s_id[e] * 8 + k, (double)s);
-      }
-      __syncthreads();
     }
   }
 };
@@ -467,17 +486,17 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) forward_
     const int* __restrict__ idx, float* __restrict__ out_color, float* __restrict__ out_alpha,
     float* __restrict__ T_last, int* __restrict__ last_pos) {
   constexpr int NP = DefaultNP<TS>::v;
-  __shared__ float4 s_pi[kChunk][4];
-  __shared__ int s_id[kChunk];
-  TileWalker<TS, NP, KIND> tw;
+  using TW = TileWalker<TS, NP, KIND>;
+  __shared__ float4 s_pi[TW::NW][kChunk][4];
+  TW tw;
   tw.init(g, blockIdx.x, offs);
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
-  tw.forward(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp);
+  tw.forward(g, prims, atlas, idx, s_pi[tw.warp], C, T, Tl, lp);
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     if (!tw.valid[p]) continue;
-    const size_t q = (size_t)tw.py[p] * g.W + tw.px[p];
+    const size_t q = (size_t)tw.py(blockIdx.x, g, p) * g.W + tw.px(blockIdx.x, g, p);
     out_color[3 * q + 0] = C[p][0];
     out_color[3 * q + 1] = C[p][1];
     out_color[3 * q + 2] = C[p][2];
@@ -496,13 +515,13 @@ __global__ void __launch_bounds__(kThreadsOf<TS>()) count_kernel(Geom g, const P
                                                                  const int* __restrict__ idx,
                                                                  unsigned long long* __restrict__ cnt) {
   constexpr int NP = DefaultNP<TS>::v;
-  __shared__ float4 s_pi[kChunk][4];
-  __shared__ int s_id[kChunk];
-  TileWalker<TS, NP, KIND> tw;
+  using TW = TileWalker<TS, NP, KIND>;
+  __shared__ float4 s_pi[TW::NW][kChunk][4];
+  TW tw;
   tw.init(g, blockIdx.x, offs);
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
-  tw.template forward<true>(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp, cnt);
+  tw.template forward<true>(g, prims, atlas, idx, s_pi[tw.warp], C, T, Tl, lp, cnt);
   if (threadIdx.x == 0) atomicAdd(cnt + 2, (unsigned long long)(tw.end - tw.start));
 }
 
@@ -513,10 +532,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward
     const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[kChunk][4];
-  __shared__ int s_id[kChunk];
-  __shared__ float s_part[TW::NW][kChunk][8];
-  __shared__ int s_kmax;
+  __shared__ float4 s_pi[TW::NW][kChunk][4];
   TW tw;
   tw.init(g, blockIdx.x, offs);
   float gC[NP][3], gA[NP], Ts[NP];
@@ -524,7 +540,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     if (tw.valid[p]) {
-      const size_t q = (size_t)tw.py[p] * g.W + tw.px[p];
+      const size_t q = (size_t)tw.py(blockIdx.x, g, p) * g.W + tw.px(blockIdx.x, g, p);
       gC[p][0] = grad_color[3 * q + 0];
       gC[p][1] = grad_color[3 * q + 1];
       gC[p][2] = grad_color[3 * q + 2];
@@ -536,7 +552,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward
       gA[p] = 0.f; Ts[p] = 1.f; lp[p] = -1;
     }
   }
-  tw.backward(g, prims, atlas, idx, s_pi, s_id, s_part, &s_kmax, gC, gA, Ts, lp, gacc);
+  tw.backward(g, prims, atlas, idx, s_pi[tw.warp], gC, gA, Ts, lp, gacc);
 }
 
 __device__ __forceinline__ double sigmoid_d(double x) {
@@ -583,7 +599,9 @@ __global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const f
 // reference's mse_loss(rendered, target) (pydiffbmp/util/loss_functions.py:20-40)
 // on rendered = C + (1 - A) * background (simple_tile_renderer.py:704-707):
 //   dL/dC = 2 (rendered - target) / (3HW),  dL/dA = -sum_c dL/dC_c * bg_c.
-// loss_out (f64, may be null) receives sum((rendered - target)^2) / (3HW).
+// loss_out (f64, may be null) receives sum((rendered - target)^2) / (3HW):
+// each warp leaves its partial in shared memory and the CTA's last warp to
+// finish its forward walk adds the CTA's sum (no barrier between the walks).
 template <int TS, int KIND>
 __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
@@ -593,16 +611,16 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
   if (skip_flag != nullptr && *skip_flag != 0) return;   // binning overflowed: leave all state untouched
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[kChunk][4];
-  __shared__ int s_id[kChunk];
-  __shared__ float s_part[TW::NW][kChunk][8];
-  __shared__ int s_kmax;
+  __shared__ float4 s_pi[TW::NW][kChunk][4];
   __shared__ float s_loss[TW::NW];
+  __shared__ unsigned s_arrived;
+  if (threadIdx.x == 0) s_arrived = 0u;
+  __syncthreads();
   TW tw;
   tw.init(g, blockIdx.x, offs);
   float C[NP][3], T[NP], Tl[NP], gC[NP][3], gA[NP];
   int lp[NP];
-  tw.forward(g, prims, atlas, idx, s_pi, s_id, C, T, Tl, lp);
+  tw.forward(g, prims, atlas, idx, s_pi[tw.warp], C, T, Tl, lp);
   const float inv = 1.f / (3.f * (float)g.H * (float)g.W);
   float lsum = 0.f;
 #pragma unroll
@@ -610,7 +628,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
     gA[p] = 0.f;
     gC[p][0] = gC[p][1] = gC[p][2] = 0.f;
     if (!tw.valid[p]) continue;
-    const size_t q = (size_t)tw.py[p] * g.W + tw.px[p];
+    const size_t q = (size_t)tw.py(blockIdx.x, g, p) * g.W + tw.px(blockIdx.x, g, p);
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
       const float bg = background ? background[3 * q + ch] : 0.f;
@@ -623,20 +641,24 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
     }
   }
   if (loss_out) {
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 16);
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 8);
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 4);
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 2);
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 1);
-    if (tw.lane == 0) s_loss[tw.warp] = lsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < TW::NW; ++w) t += s_loss[w];
-      atomicAdd(loss_out, t * (double)inv);
+    lsum += __shfl_xor_sync(kFull, lsum, 16);
+    lsum += __shfl_xor_sync(kFull, lsum, 8);
+    lsum += __shfl_xor_sync(kFull, lsum, 4);
+    lsum += __shfl_xor_sync(kFull, lsum, 2);
+    lsum += __shfl_xor_sync(kFull, lsum, 1);
+    if (tw.lane == 0) {
+      s_loss[tw.warp] = lsum;
+      __threadfence_block();
+      if (atomicAdd(&s_arrived, 1u) == (unsigned)(TW::NW - 1)) {
+        __threadfence_block();
+        const volatile float* sl = s_loss;
+        double t = 0.0;
+        for (int w = 0; w < TW::NW; ++w) t += sl[w];
+        atomicAdd(loss_out, t * (double)inv);
+      }
     }
   }
-  tw.backward(g, prims, atlas, idx, s_pi, s_id, s_part, &s_kmax, gC, gA, Tl, lp, gacc);
+  tw.backward(g, prims, atlas, idx, s_pi[tw.warp], gC, gA, Tl, lp, gacc);
 }
 
 // ---------------------------------------------------------------------------
