@@ -401,7 +401,7 @@ def main():
                                "one fit iteration per step (device binning, fused fwd+L2+bwd, Adam) with FP16-pair atlas "
                                "storage and FP32 arithmetic, CUDA-graph replay",
                    "canvas": [spec.H, spec.W], "N": spec.N, "tile_size": 32, "t_stop": job.cfg.t_stop,
-                   "l2": "per-step working set (target 50 MB + tile lists/sort buffers) exceeds the 126 MB L2",
+                   "l2": "per-step working set (target 50 MB + background 50 MB + tile lists 28 MB) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world}", "tile_list_entries": L, "replayed_steps": replayed},
         "plain_fp32": {"iters_per_s": world * args.steps / t_plain, "ms_per_step": t_plain / args.steps * 1e3,
                        "what": "unfused forward + torch L2 gradient + backward, FP32 atlas, graph replay"},
@@ -422,9 +422,9 @@ def main():
         "e2e": {"value": world * args.steps / t_e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 8,
                 "what": "public API: params H2D from pinned host, ImageFitter.step(), loss D2H, synchronised"},
-        "gpu_launches": 7 * args.steps,
-        "gpu_launches_note": "ours per step: prepare, emit, fill_tail, tile_offsets, fused, adam, step_increment "
-                             "(+ CUB scan and radix-sort kernels)",
+        "gpu_launches": 6 * args.steps,
+        "gpu_launches_note": "ours per step: prepare, bin_rows<count>, bin_rows<write>, fused, adam, step_increment "
+                             "(+ the two kernels of one CUB exclusive scan over the tile counts)",
         "clocks": clocks,
     }
     if args.serving_jobs > 0:

@@ -1,6 +1,10 @@
 // Device binning: per-primitive preparation, primitive -> tile rectangles,
-// (tile, primitive) key emission and a stable radix sort by tile, producing
-// the reference's CSR tile lists without any host round trip.
+// then CSR tile lists built row by row without a sort: for each tile row a
+// group of CTAs walks the primitives in index order, compacts those whose
+// rectangle touches the group's tiles, and each warp counts (first pass) or
+// writes (second pass) the entries of its own tile.  Lists therefore come out
+// in ascending primitive order per tile, as the reference's per-tile nonzero()
+// gives them, with no host round trip.
 //
 // This translation unit is compiled WITHOUT fast-math: the world-space bbox
 // must reproduce the reference's float32 torch element-wise arithmetic
@@ -137,7 +141,7 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
                                const float* __restrict__ rot, const float* __restrict__ opac,
                                const float* __restrict__ colors, const int* __restrict__ sel,
                                const float* __restrict__ tbbox, int bin_mode, PrimInfo* __restrict__ out,
-                               int4* __restrict__ rects, long long* __restrict__ counts) {
+                               int4* __restrict__ rects) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= g.N) return;
   const float mx = means2D[2 * n], my = means2D[2 * n + 1];
@@ -203,69 +207,126 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
       sx = make_int2(1, 0); sy = make_int2(1, 0);
     }
   }
-  const long long w = max(0, sx.y - sx.x + 1), h = max(0, sy.y - sy.x + 1);
   rects[n] = make_int4(sx.x, sx.y, sy.x, sy.y);
-  counts[n] = w * h;
 }
 
-// One warp per primitive writes (tile id, primitive id) for every tile of its
-// rectangle, in row-major tile order, at its exclusive-scan offset.
-__global__ void emit_kernel(Geom g, const int4* __restrict__ rects, const long long* __restrict__ offs,
-                            long long cap, unsigned* __restrict__ keys, unsigned* __restrict__ vals) {
-  const long long total = offs[g.N];
-  if (total > cap) return;
-  const int lane = threadIdx.x & 31;
-  for (int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; n < g.N; n += (gridDim.x * blockDim.x) >> 5) {
-    const long long o = offs[n], cnt = offs[n + 1] - o;
-    if (cnt == 0) continue;
-    const int4 rc = rects[n];
-    const int w = rc.y - rc.x + 1;
-    for (long long j = lane; j < cnt; j += 32) {
-      const int dy = (int)(j / w), dx = (int)(j - (long long)dy * w);
-      keys[o + j] = (unsigned)((rc.z + dy) * g.tilesX + rc.x + dx);
-      vals[o + j] = (unsigned)n;
+// Tile lists, one CTA per (tile row, group of kBinGroup tiles, primitive
+// slice), one warp per tile.  The CTA walks the primitives of its slice in
+// index order in chunks of kBinThreads, compacts those whose rectangle covers
+// its row and overlaps its tile group, and each warp scans the compacted
+// chunk for rectangles containing its tile: with WRITE=false it counts them
+// into counts[t * S + slice]; with WRITE=true it writes their ids from
+// offs[t * S + slice] on.  The exclusive scan of the counts is tile-major and
+// slice-minor, so a tile's entries come out in ascending primitive order.
+// The WRITE pass also publishes tile_offsets, L and the overflow flag, and
+// leaves the outputs untouched when L exceeds the capacity.
+constexpr int kBinThreads = 512;
+constexpr int kBinGroup = kBinThreads / 32;
+
+struct BinGrid {
+  int groups;   // tile groups per row
+  int slices;   // primitive slices
+  int span;     // primitives per slice (multiple of kBinThreads)
+  long long ctas;
+};
+
+// Enough slices to give every SM several CTAs, never a slice below one chunk.
+static inline BinGrid bin_grid(int N, int tilesX, int tilesY) {
+  BinGrid b;
+  b.groups = (tilesX + kBinGroup - 1) / kBinGroup;
+  const long long base = (long long)b.groups * tilesY;
+  const int chunks = N > 0 ? (N + kBinThreads - 1) / kBinThreads : 1;
+  const long long want = (148 * 8 + base - 1) / base;
+  b.slices = (int)(want < chunks ? want : chunks);
+  if (b.slices < 1) b.slices = 1;
+  const int per = (chunks + b.slices - 1) / b.slices;
+  b.span = per * kBinThreads;
+  b.slices = N > 0 ? (N + b.span - 1) / b.span : 1;
+  b.ctas = base * b.slices;
+  return b;
+}
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid bg, const int4* __restrict__ rects,
+                                                               long long* __restrict__ counts,
+                                                               const long long* __restrict__ offs, long long cap,
+                                                               int* __restrict__ indices,
+                                                               int* __restrict__ tile_offsets,
+                                                               int* __restrict__ total_out,
+                                                               int* __restrict__ overflow_out) {
+  __shared__ int s_id[kBinThreads], s_x0[kBinThreads], s_x1[kBinThreads];
+  __shared__ int s_wcnt[kBinGroup];
+  const int slice = blockIdx.x % bg.slices;
+  const int rg = blockIdx.x / bg.slices;
+  const int ty = rg / bg.groups;
+  const int gx0 = (rg - ty * bg.groups) * kBinGroup, gx1 = min(gx0 + kBinGroup - 1, g.tilesX - 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tx = gx0 + warp;
+  const bool has_tile = tx <= gx1;
+  const int t = ty * g.tilesX + tx;
+  const long long slot = (long long)t * bg.slices + slice;
+  const long long nslots = (long long)g.T * bg.slices;
+  const unsigned lt = (1u << lane) - 1u;
+  long long cur = 0;
+  if (WRITE) {
+    const long long L = offs[nslots];
+    const bool first = blockIdx.x == 0 && threadIdx.x == 0;
+    if (first) {
+      if (total_out) *total_out = (int)min(L, (long long)INT_MAX);
+      if (overflow_out) *overflow_out = (L > cap) ? 1 : 0;
     }
+    if (L > cap) return;
+    if (first) tile_offsets[g.T] = (int)L;
+    if (has_tile) {
+      cur = offs[slot];
+      if (lane == 0 && slice == 0) tile_offsets[t] = (int)cur;
+    }
+  } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counts[nslots] = 0;
   }
-}
-
-// Entries [L, cap) get the sentinel key T so they sort behind every tile.
-__global__ void fill_tail_kernel(const long long* __restrict__ total_p, int N, long long cap, unsigned sentinel,
-                                 unsigned* __restrict__ keys, unsigned* __restrict__ vals) {
-  const long long L = total_p[N];
-  if (L > cap) return;
-  for (long long i = L + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
-    keys[i] = sentinel;
-    vals[i] = 0u;
+  const int lo = slice * bg.span, hi = min(g.N, lo + bg.span);
+  int4 rc = make_int4(1, 0, 1, 0);
+  if (lo + (int)threadIdx.x < hi) rc = rects[lo + threadIdx.x];
+  for (int base = lo; base < hi; base += kBinThreads) {
+    const int n = base + threadIdx.x;
+    // prefetch the next chunk's rectangle while this one is processed
+    int4 rn = make_int4(1, 0, 1, 0);
+    if (n + kBinThreads < hi) rn = rects[n + kBinThreads];
+    const bool f = n < hi && rc.x <= rc.y && rc.z <= ty && ty <= rc.w && rc.x <= gx1 && rc.y >= gx0;
+    const unsigned b = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) s_wcnt[warp] = __popc(b);
+    __syncthreads();
+    int wbase = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kBinGroup; ++w) {
+      const int c = s_wcnt[w];
+      wbase += (w < warp) ? c : 0;
+      total += c;
+    }
+    if (f) {
+      const int p = wbase + __popc(b & lt);
+      s_id[p] = n; s_x0[p] = rc.x; s_x1[p] = rc.y;
+    }
+    __syncthreads();
+    if (has_tile) {
+      for (int j = lane; j < ((total + 31) & ~31); j += 32) {
+        const bool in = j < total && s_x0[j] <= tx && tx <= s_x1[j];
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (WRITE && in) indices[cur + __popc(m & lt)] = s_id[j];
+        cur += __popc(m);
+      }
+    }
+    __syncthreads();   // the compacted chunk is reused by the next iteration
+    rc = rn;
   }
-}
-
-// offsets[t] = first position whose sorted key >= t (t = 0..T).
-__global__ void tile_offsets_kernel(const long long* __restrict__ total_p, int N, long long cap, int T,
-                                    const unsigned* __restrict__ skeys, int* __restrict__ offsets,
-                                    int* __restrict__ total_out, int* __restrict__ overflow_out) {
-  const long long L = total_p[N];
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) {
-    if (total_out) *total_out = (int)min(L, (long long)INT_MAX);
-    if (overflow_out) *overflow_out = (L > cap) ? 1 : 0;
-  }
-  if (L > cap || t > T) return;
-  long long lo = 0, hi = L;
-  while (lo < hi) {
-    const long long mid = (lo + hi) >> 1;
-    if (skeys[mid] < (unsigned)t) lo = mid + 1; else hi = mid;
-  }
-  offsets[t] = (int)lo;
+  if (!WRITE && has_tile && lane == 0) counts[slot] = cur;
 }
 
 // ---------------------------------------------------------------------------
 struct BinWorkspace {
-  int4* rects;
-  long long* counts;   // N+1
-  long long* offs;     // N+1
-  unsigned* keys_in;
-  unsigned* vals_in;
-  unsigned* keys_out;
+  int4* rects;         // N tile rectangles (x0, x1, y0, y1)
+  long long* counts;   // T*S+1 entries per (tile, primitive slice)
+  long long* offs;     // exclusive prefix of counts
   void* cub_tmp;
   size_t cub_bytes;
   size_t total;
@@ -273,28 +334,16 @@ struct BinWorkspace {
 
 static inline size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
-static int key_bits(int T) {
-  int bits = 0;
-  while ((1u << bits) <= (unsigned)T && bits < 32) ++bits;
-  return bits < 1 ? 1 : bits;
-}
-
-static BinWorkspace layout_ws(void* base, int N, int T, long long cap, bool query, size_t* needed) {
+static BinWorkspace layout_ws(void* base, int N, int T, long long nslots, bool query, size_t* needed) {
   BinWorkspace w{};
-  size_t scan_bytes = 0, sort_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long*)nullptr, (long long*)nullptr, N + 1);
-  if (cap > 0)
-    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (unsigned*)nullptr, (unsigned*)nullptr,
-                                    (unsigned*)nullptr, (unsigned*)nullptr, (int)cap, 0, key_bits(T));
-  w.cub_bytes = align_up(scan_bytes > sort_bytes ? scan_bytes : sort_bytes);
+  size_t scan_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long*)nullptr, (long long*)nullptr, nslots + 1);
+  w.cub_bytes = align_up(scan_bytes);
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes); return o; };
-  const size_t o_rects = take(sizeof(int4) * (size_t)N);
-  const size_t o_counts = take(sizeof(long long) * (size_t)(N + 1));
-  const size_t o_offs = take(sizeof(long long) * (size_t)(N + 1));
-  const size_t o_kin = take(sizeof(unsigned) * (size_t)cap);
-  const size_t o_vin = take(sizeof(unsigned) * (size_t)cap);
-  const size_t o_kout = take(sizeof(unsigned) * (size_t)cap);
+  const size_t o_rects = take(sizeof(int4) * (size_t)(N > 0 ? N : 1));
+  const size_t o_counts = take(sizeof(long long) * (size_t)(nslots + 1));
+  const size_t o_offs = take(sizeof(long long) * (size_t)(nslots + 1));
   const size_t o_cub = take(w.cub_bytes);
   w.total = off;
   if (needed) *needed = off;
@@ -303,17 +352,16 @@ static BinWorkspace layout_ws(void* base, int N, int T, long long cap, bool quer
     w.rects = reinterpret_cast<int4*>(b + o_rects);
     w.counts = reinterpret_cast<long long*>(b + o_counts);
     w.offs = reinterpret_cast<long long*>(b + o_offs);
-    w.keys_in = reinterpret_cast<unsigned*>(b + o_kin);
-    w.vals_in = reinterpret_cast<unsigned*>(b + o_vin);
-    w.keys_out = reinterpret_cast<unsigned*>(b + o_kout);
     w.cub_tmp = b + o_cub;
   }
   return w;
 }
 
-size_t bin_workspace_bytes(int N, int T, long long cap) {
+size_t bin_workspace_bytes(int N, int T, int tilesX, int tilesY, long long cap) {
+  (void)cap;   // the row binning needs no scratch per list entry
+  const BinGrid bg = bin_grid(N, tilesX, tilesY);
   size_t need = 0;
-  layout_ws(nullptr, N, T, cap, true, &need);
+  layout_ws(nullptr, N, T, (long long)T * bg.slices, true, &need);
   return need;
 }
 
@@ -400,7 +448,7 @@ int launch_prepare(const Geom& g, const float* means2D, const float* radii, cons
                    const float* colors, const int* sel, PrimInfo* out, cudaStream_t st) {
   if (g.N == 0) return DBMP_OK;
   prepare_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(g, means2D, radii, rot, opac, colors, sel, nullptr, 0,
-                                                    out, nullptr, nullptr);
+                                                    out, nullptr);
   DBMP_CHECK_LAUNCH("prepare_kernel");
   return DBMP_OK;
 }
@@ -409,39 +457,30 @@ int launch_bin(const Geom& g, int bin_mode, const float* means2D, const float* r
                const float* opac, const float* colors, const int* sel, const float* tbbox, PrimInfo* prim_info,
                int* tile_offsets, int* tile_indices, long long cap, int* total_out, int* overflow_out,
                void* ws, size_t ws_bytes, cudaStream_t st) {
+  const BinGrid bg = bin_grid(g.N, g.tilesX, g.tilesY);
+  const long long nslots = (long long)g.T * bg.slices;
   size_t need = 0;
-  BinWorkspace w = layout_ws(ws, g.N, g.T, cap, false, &need);
+  BinWorkspace w = layout_ws(ws, g.N, g.T, nslots, false, &need);
   if (ws_bytes < need) {
     set_error("dbmp_bin: workspace of %zu bytes is smaller than the %zu bytes required", ws_bytes, need);
     return DBMP_ERR_CAPACITY;
   }
-  const int N = g.N;
-  cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(long long) * (N + 1), st);
-  if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(counts)");
-  if (N > 0) {
-    prepare_kernel<<<(N + 255) / 256, 256, 0, st>>>(g, means2D, radii, rot, opac, colors, sel, tbbox, bin_mode,
-                                                    prim_info, w.rects, w.counts);
+  if (g.N > 0) {
+    prepare_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(g, means2D, radii, rot, opac, colors, sel, tbbox, bin_mode,
+                                                      prim_info, w.rects);
     DBMP_CHECK_LAUNCH("prepare_kernel");
   }
+  if (bg.ctas > 0x7fffffffll) { set_error("dbmp_bin: canvas and primitive count too large"); return DBMP_ERR_INVALID; }
+  const int grid = (int)bg.ctas;   // (tile row, tile group, primitive slice) triples
+  bin_rows_kernel<false><<<grid, kBinThreads, 0, st>>>(g, bg, w.rects, w.counts, nullptr, cap, nullptr, nullptr,
+                                                       nullptr, nullptr);
+  DBMP_CHECK_LAUNCH("bin_rows_kernel<count>");
   size_t tmp = w.cub_bytes;
-  e = cub::DeviceScan::ExclusiveSum(w.cub_tmp, tmp, w.counts, w.offs, N + 1, st);
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(w.cub_tmp, tmp, w.counts, w.offs, nslots + 1, st);
   if (e != cudaSuccess) return cuda_status(e, "cub::DeviceScan::ExclusiveSum");
-  if (cap > 0) {
-    if (N > 0) {
-      const int blocks = (N * 32 + 255) / 256 < 148 * 16 ? (N * 32 + 255) / 256 : 148 * 16;
-      emit_kernel<<<blocks, 256, 0, st>>>(g, w.rects, w.offs, cap, w.keys_in, w.vals_in);
-      DBMP_CHECK_LAUNCH("emit_kernel");
-    }
-    fill_tail_kernel<<<148 * 4, 256, 0, st>>>(w.offs, N, cap, (unsigned)g.T, w.keys_in, w.vals_in);
-    DBMP_CHECK_LAUNCH("fill_tail_kernel");
-    tmp = w.cub_bytes;
-    e = cub::DeviceRadixSort::SortPairs(w.cub_tmp, tmp, w.keys_in, w.keys_out, w.vals_in,
-                                        reinterpret_cast<unsigned*>(tile_indices), (int)cap, 0, key_bits(g.T), st);
-    if (e != cudaSuccess) return cuda_status(e, "cub::DeviceRadixSort::SortPairs");
-  }
-  tile_offsets_kernel<<<(g.T + 1 + 255) / 256, 256, 0, st>>>(w.offs, N, cap, g.T, w.keys_out, tile_offsets,
-                                                             total_out, overflow_out);
-  DBMP_CHECK_LAUNCH("tile_offsets_kernel");
+  bin_rows_kernel<true><<<grid, kBinThreads, 0, st>>>(g, bg, w.rects, nullptr, w.offs, cap, tile_indices,
+                                                      tile_offsets, total_out, overflow_out);
+  DBMP_CHECK_LAUNCH("bin_rows_kernel<write>");
   return DBMP_OK;
 }
 

@@ -22,7 +22,7 @@ int cuda_status(cudaError_t e, const char* what) {
 }
 
 // launchers (binning.cu, raster.cu)
-size_t bin_workspace_bytes(int N, int T, long long cap);
+size_t bin_workspace_bytes(int N, int T, int tilesX, int tilesY, long long cap);
 size_t atlas_bytes(int P, int Ht, int Wt, int kind);
 int launch_template_bboxes(const float* tmpl, int P, int Ht, int Wt, float* out, cudaStream_t st);
 int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st);
@@ -145,7 +145,7 @@ size_t dbmp_bin_workspace_bytes(const dbmp_canvas* cv, long long capacity) {
   Geom g;
   if (make_geom(cv, &g, "dbmp_bin_workspace_bytes") != DBMP_OK) return 0;
   if (capacity < 0) capacity = 0;
-  return bin_workspace_bytes(g.N, g.T, capacity);
+  return bin_workspace_bytes(g.N, g.T, g.tilesX, g.tilesY, capacity);
 }
 
 int dbmp_prepare(const dbmp_canvas* cv, const float* means2D, const float* radii, const float* rotations,

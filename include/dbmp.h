@@ -92,7 +92,8 @@ int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* o
 size_t dbmp_atlas_bytes(int P, int Ht, int Wt, int kind);
 int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, void* out, void* stream);
 
-/* Scratch bytes that dbmp_bin needs for `capacity` tile-list entries. */
+/* Scratch bytes that dbmp_bin needs (per primitive and per tile; the
+ * capacity argument is accepted for compatibility and does not change it). */
 size_t dbmp_bin_workspace_bytes(const dbmp_canvas* cv, long long capacity);
 /* Bytes of the per-primitive record array written by dbmp_bin / dbmp_prepare. */
 size_t dbmp_prim_info_bytes(int num_prims);
@@ -105,8 +106,9 @@ int dbmp_prepare(const dbmp_canvas* cv, const float* means2D, const float* radii
                  const float* rotations, const float* opacities, const float* colors,
                  const int32_t* sel, void* prim_info, void* stream);
 
-/* Device binning: preparation + per-primitive tile rectangles + stable key
- * sort by tile -> CSR tile lists.  Writes prim_info, tile_offsets (T+1),
+/* Device binning: preparation + per-primitive tile rectangles -> CSR tile
+ * lists, built per tile row in primitive order (no sort).  Writes prim_info,
+ * tile_offsets (T+1),
  * tile_indices (first L of `capacity` entries) and *total_out (device int32,
  * = L).  When L > capacity the lists are not written, *total_out still holds
  * L and *overflow_out (device int32, may be null) is set to 1; call again with

@@ -41,7 +41,11 @@ def test_num_tiles_and_workspace_query():
     from diffbmp_b200._lib import lib
     assert lib.dbmp_num_tiles(ctypes.byref(canvas())) == 64
     assert lib.dbmp_num_tiles(ctypes.byref(canvas(height=200, width=136, tile_size=16))) == 13 * 9
-    assert lib.dbmp_bin_workspace_bytes(ctypes.byref(canvas()), 1 << 20) > 3 * 4 * (1 << 20)
+    # per-primitive rectangles + per-tile counts and offsets; independent of the list capacity
+    ws = lib.dbmp_bin_workspace_bytes(ctypes.byref(canvas()), 1 << 20)
+    c = canvas()
+    assert ws >= 16 * c.num_prims + 2 * 8 * (64 + 1)
+    assert ws == lib.dbmp_bin_workspace_bytes(ctypes.byref(canvas()), 0)
     assert lib.dbmp_prim_info_bytes(10) == 640
 
 
