@@ -166,13 +166,21 @@ class ImageFitter:
         self.steps_enqueued += 1
 
     def capture(self):
-        """Captures one iteration in a CUDA graph; later step() calls replay it."""
+        """Captures one iteration in a CUDA graph; later step() calls replay it.
+
+        Uses capture_begin/capture_end directly: the torch.cuda.graph context
+        manager also synchronises the device, runs the garbage collector and
+        empties the allocator cache on every capture, which costs a serving
+        loop up to hundreds of milliseconds per admitted job."""
         s = torch.cuda.Stream(self.device)
         s.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
         with torch.cuda.stream(s):
-            g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=s):
+            g.capture_begin()
+            try:
                 self._enqueue()
+            finally:
+                g.capture_end()
         torch.cuda.current_stream().wait_stream(s)
         self.graph = g
 

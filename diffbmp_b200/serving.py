@@ -106,6 +106,8 @@ class Server:
         return _Slot(req, f, stream, now)
 
     def run(self, requests: List[JobRequest], realtime=True) -> List[JobResult]:
+        """Serves `requests`.  realtime: admit each at its arrival time (else
+        all are queued at the start and latencies count from 0)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         active: List[_Slot] = []
         results: List[JobResult] = []
@@ -139,7 +141,9 @@ class Server:
                         replayed = f.sync()
                         loss = f.loss()
                     params = {k: v.detach().clone() for k, v in f.params().items()} if self.keep_params else None
-                    results.append(JobResult(slot.req.job_id, slot.req.arrival, slot.admitted, clock(), loss,
+                    # without realtime arrivals every request is queued at the start
+                    arrival = slot.req.arrival if realtime else 0.0
+                    results.append(JobResult(slot.req.job_id, arrival, slot.admitted, clock(), loss,
                                              replayed, params))
                     active.remove(slot)
                     used -= slot.nbytes
