@@ -67,7 +67,9 @@ struct Sample {
 // inverse affine is linear, so pixel p is pixel 0 plus a multiple of a column
 // of A) and whether the pixel can yield a fragment (live, inside the cull
 // square, inside [0,W-1]x[0,H-1]).
-template <int NP, class L>
+// FAST: the warp footprint lies inside the cull square and its texel-space
+// box inside the template (with margin), so every pixel passes both tests.
+template <int NP, class L, bool FAST>
 __device__ __forceinline__ void entry_coords(const Geom& g, const float4& g0, const float4& g1, bool inside,
                                              const float (&pxf)[NP], const float (&pyf)[NP],
                                              const bool (&live)[NP], Sample (&s)[NP]) {
@@ -79,13 +81,25 @@ __device__ __forceinline__ void entry_coords(const Geom& g, const float4& g0, co
     float tx = tx0, ty = ty0;
     if (L::ox(p)) { tx = fmaf((float)L::ox(p), g1.x, tx); ty = fmaf((float)L::ox(p), g1.z, ty); }
     if (L::oy(p)) { tx = fmaf((float)L::oy(p), g1.y, tx); ty = fmaf((float)L::oy(p), g1.w, ty); }
-    bool cull_ok = inside;
-    if (!inside) cull_ok = !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
-    const bool in_rng = tx >= 0.f && tx <= g.wm1 && ty >= 0.f && ty <= g.hm1;
-    s[p].ok = live[p] && cull_ok && in_rng;
+    if (FAST) {
+      s[p].ok = live[p];
+    } else {
+      bool cull_ok = inside;
+      if (!inside) cull_ok = !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+      const bool in_rng = tx >= 0.f && tx <= g.wm1 && ty >= 0.f && ty <= g.hm1;
+      s[p].ok = live[p] && cull_ok && in_rng;
+    }
     s[p].tx = tx;
     s[p].ty = ty;
   }
+}
+
+template <int NP, class L>
+__device__ __forceinline__ void entry_coords_any(const Geom& g, const float4& g0, const float4& g1, bool inside,
+                                                 bool fast, const float (&pxf)[NP], const float (&pyf)[NP],
+                                                 const bool (&live)[NP], Sample (&s)[NP]) {
+  if (fast) entry_coords<NP, L, true>(g, g0, g1, inside, pxf, pyf, live, s);
+  else entry_coords<NP, L, false>(g, g0, g1, inside, pxf, pyf, live, s);
 }
 
 // Phase 2 for one pixel: sampling position and texel fetch (texel 0 of the
@@ -120,6 +134,7 @@ __device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
 struct ChunkMasks {
   unsigned todo;     // entries the warp composites
   unsigned inside;   // footprint entirely inside the entry's cull square
+  unsigned fast;     // ... and its texel-space box inside the template
   unsigned clear;    // clearance grid shows no fragment (skipped unless counting)
   unsigned miss;     // footprint misses the cull square
 };
@@ -174,7 +189,7 @@ struct TileWalker {
   __device__ __forceinline__ ChunkMasks stage(const Geom& g, const PrimInfo* __restrict__ prims,
                                               const int* __restrict__ idx, const unsigned char* __restrict__ grid,
                                               int base, int stop, float4 (*w)[4], int* my_id) {
-    bool keep = false, inside = false, clear = false, miss = false;
+    bool keep = false, inside = false, fast = false, clear = false, miss = false;
     int id = -1;
     __syncwarp();   // every lane is done with the previous chunk's records
     const int pos = base + lane;
@@ -194,6 +209,16 @@ struct TileWalker {
             keep = KEEP_CLEAR || !clear;
             if (keep) {
               inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
+              if (inside && toff != kSolid) {
+                // texel box of the footprint: centre +- |A| (half extents), plus
+                // 0.05 texel for the rounding of the per-pixel coordinates
+                const float dx = fcx - g0.x, dy = fcy - g0.y;
+                const float cx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
+                const float cy = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
+                const float ex = fmaf(fabsf(g1.x), g.fhx, fmaf(fabsf(g1.y), g.fhy, 0.05f));
+                const float ey = fmaf(fabsf(g1.z), g.fhx, fmaf(fabsf(g1.w), g.fhy, 0.05f));
+                fast = cx - ex >= 0.f && cx + ex <= g.wm1 && cy - ey >= 0.f && cy + ey <= g.hm1;
+              }
               w[lane][0] = g0;
               w[lane][1] = g1;
               w[lane][2] = __ldg(r + 2);
@@ -210,6 +235,7 @@ struct TileWalker {
     ChunkMasks m;
     m.todo = __ballot_sync(kFull, keep);
     m.inside = __ballot_sync(kFull, inside);
+    m.fast = __ballot_sync(kFull, fast);
     m.clear = KEEP_CLEAR ? __ballot_sync(kFull, clear) : 0u;
     m.miss = KEEP_CLEAR ? __ballot_sync(kFull, miss) : 0u;
     return m;
@@ -264,7 +290,7 @@ struct TileWalker {
         Sample s[NP];
         float m[NP];
         if (toff != kSolid) {
-          entry_coords<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, pxf, pyf, live, s);
+          entry_coords_any<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf, live, s);
           bool any[NP];
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
@@ -301,17 +327,15 @@ struct TileWalker {
         for (int p = 0; p < NP; ++p) {
           const bool frag = s[p].ok && m[p] > 1e-6f;
           if (STATS) { n_frag += frag; n_depth[p] += frag; }
-          if (__any_sync(kFull, frag)) {
-            const float a = frag ? g2.x * m[p] : 0.f;
-            const float wt = T[p] * a;
-            C[p][0] = fmaf(wt, g2.y, C[p][0]);
-            C[p][1] = fmaf(wt, g2.z, C[p][1]);
-            C[p][2] = fmaf(wt, g2.w, C[p][2]);
-            Tl[p] = frag ? T[p] : Tl[p];
-            lp[p] = frag ? pos : lp[p];
-            T[p] *= fmaxf(1.f - a, 0.f);
-            live[p] = live[p] && !(T[p] < g.t_stop);
-          }
+          const float a = frag ? g2.x * m[p] : 0.f;
+          const float wt = T[p] * a;
+          C[p][0] = fmaf(wt, g2.y, C[p][0]);
+          C[p][1] = fmaf(wt, g2.z, C[p][1]);
+          C[p][2] = fmaf(wt, g2.w, C[p][2]);
+          Tl[p] = frag ? T[p] : Tl[p];
+          lp[p] = frag ? pos : lp[p];
+          T[p] *= fmaxf(1.f - a, 0.f);
+          live[p] = live[p] && !(T[p] < g.t_stop);
           local_done = local_done && !live[p];
         }
         if (__all_sync(kFull, local_done)) { warp_done = true; break; }
@@ -386,7 +410,7 @@ struct TileWalker {
         float m[NP], gx[NP], gy[NP];
         bool anyp[NP];
         if (toff != kSolid) {
-          entry_coords<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, pxf, pyf, live, s);
+          entry_coords_any<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf, live, s);
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
             anyp[p] = __any_sync(kFull, s[p].ok);
