@@ -1,6 +1,6 @@
 // Forward / backward / fused tile compositing kernels.
 //
-// One CTA owns one tile of TS x TS pixels; each thread owns NP pixels
+// A tile of TS x TS pixels is walked by NW warps (one or more CTAs); each thread owns NP pixels
 // (NP = 4, 2 or 1) of a compact warp footprint (16x8, 16x4 or 8x4 pixels) so
 // that a primitive's square cull is mostly warp-uniform and the warp's texel
 // fetches stay close together in the atlas.
@@ -146,13 +146,17 @@ struct TileWalker {
   static constexpr int NW = L::NW;
   static constexpr bool kGrid = KIND != ATLAS_F32;   // packed atlases carry a clearance grid
 
-  int warp, lane, start, end;
+  int warp, lw, lane, start, end;   // warp: index within the tile, lw: within the CTA
   float pxf[NP], pyf[NP];
   bool valid[NP];
   float fx0, fx1, fy0, fy1, fcx, fcy;
 
-  __device__ __forceinline__ void init(const Geom& g, int tile, const int* __restrict__ offs) {
-    warp = threadIdx.x >> 5;
+  // tile: the CTA's tile; part: which group of warps of the tile the CTA runs
+  // (a CTA holds kCtaWarps of the tile's NW warps).
+  __device__ __forceinline__ void init(const Geom& g, int tile, int part, int cta_warps,
+                                       const int* __restrict__ offs) {
+    lw = threadIdx.x >> 5;
+    warp = part * cta_warps + lw;
     lane = threadIdx.x & 31;
     const int tx = tile % g.tilesX, ty = tile / g.tilesX;
     start = __ldg(offs + tile);
@@ -491,16 +495,24 @@ struct TileWalker {
   }
 };
 
-template <int TS> constexpr int kThreadsOf() { return Layout<TS, DefaultNP<TS>::v>::NT; }
-// Resident CTAs per SM the register allocation is bounded for (walk kernels).
-#ifndef DBMP_MINBLOCKS256
-#define DBMP_MINBLOCKS256 3
+// CTA shape of the walk kernels: a CTA runs kCtaWarps warps of one tile (the
+// warps walk independently, so a tile may be split over several CTAs, which
+// lets an SM refill as soon as a few warps finish); kParts CTAs per tile.
+// Registers are bounded for kWarpsPerSM resident warps per SM.
+#ifndef DBMP_CTA_WARPS
+#define DBMP_CTA_WARPS 4
 #endif
-#ifndef DBMP_MINBLOCKS512
-#define DBMP_MINBLOCKS512 2
+#ifndef DBMP_WARPS_PER_SM
+#define DBMP_WARPS_PER_SM 32
 #endif
+template <int TS> constexpr int kTileWarps() { return Layout<TS, DefaultNP<TS>::v>::NW; }
+template <int TS> constexpr int kCtaWarps() {
+  return kTileWarps<TS>() < DBMP_CTA_WARPS ? kTileWarps<TS>() : DBMP_CTA_WARPS;
+}
+template <int TS> constexpr int kParts() { return kTileWarps<TS>() / kCtaWarps<TS>(); }
+template <int TS> constexpr int kThreadsOf() { return kCtaWarps<TS>() * 32; }
 template <int TS> constexpr int kBlocksPerSM() {
-  return kThreadsOf<TS>() >= 1024 ? 1 : kThreadsOf<TS>() >= 512 ? DBMP_MINBLOCKS512 : DBMP_MINBLOCKS256;
+  return DBMP_WARPS_PER_SM / kCtaWarps<TS>() > 0 ? DBMP_WARPS_PER_SM / kCtaWarps<TS>() : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -511,16 +523,17 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) forward_
     float* __restrict__ T_last, int* __restrict__ last_pos) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[TW::NW][kChunk][4];
+  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
   TW tw;
-  tw.init(g, blockIdx.x, offs);
+  const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
+  tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
-  tw.forward(g, prims, atlas, idx, s_pi[tw.warp], C, T, Tl, lp);
+  tw.forward(g, prims, atlas, idx, s_pi[tw.lw], C, T, Tl, lp);
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     if (!tw.valid[p]) continue;
-    const size_t q = (size_t)tw.py(blockIdx.x, g, p) * g.W + tw.px(blockIdx.x, g, p);
+    const size_t q = (size_t)tw.py(tile, g, p) * g.W + tw.px(tile, g, p);
     out_color[3 * q + 0] = C[p][0];
     out_color[3 * q + 1] = C[p][1];
     out_color[3 * q + 2] = C[p][2];
@@ -540,13 +553,14 @@ __global__ void __launch_bounds__(kThreadsOf<TS>()) count_kernel(Geom g, const P
                                                                  unsigned long long* __restrict__ cnt) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[TW::NW][kChunk][4];
+  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
   TW tw;
-  tw.init(g, blockIdx.x, offs);
+  const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
+  tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
-  tw.template forward<true>(g, prims, atlas, idx, s_pi[tw.warp], C, T, Tl, lp, cnt);
-  if (threadIdx.x == 0) atomicAdd(cnt + 2, (unsigned long long)(tw.end - tw.start));
+  tw.template forward<true>(g, prims, atlas, idx, s_pi[tw.lw], C, T, Tl, lp, cnt);
+  if (threadIdx.x == 0 && part == 0) atomicAdd(cnt + 2, (unsigned long long)(tw.end - tw.start));
 }
 
 template <int TS, int KIND>
@@ -556,15 +570,16 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward
     const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[TW::NW][kChunk][4];
+  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
   TW tw;
-  tw.init(g, blockIdx.x, offs);
+  const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
+  tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float gC[NP][3], gA[NP], Ts[NP];
   int lp[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     if (tw.valid[p]) {
-      const size_t q = (size_t)tw.py(blockIdx.x, g, p) * g.W + tw.px(blockIdx.x, g, p);
+      const size_t q = (size_t)tw.py(tile, g, p) * g.W + tw.px(tile, g, p);
       gC[p][0] = grad_color[3 * q + 0];
       gC[p][1] = grad_color[3 * q + 1];
       gC[p][2] = grad_color[3 * q + 2];
@@ -576,7 +591,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward
       gA[p] = 0.f; Ts[p] = 1.f; lp[p] = -1;
     }
   }
-  tw.backward(g, prims, atlas, idx, s_pi[tw.warp], gC, gA, Ts, lp, gacc);
+  tw.backward(g, prims, atlas, idx, s_pi[tw.lw], gC, gA, Ts, lp, gacc);
 }
 
 __device__ __forceinline__ double sigmoid_d(double x) {
@@ -635,16 +650,17 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
   if (skip_flag != nullptr && *skip_flag != 0) return;   // binning overflowed: leave all state untouched
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[TW::NW][kChunk][4];
-  __shared__ float s_loss[TW::NW];
+  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
+  __shared__ float s_loss[kCtaWarps<TS>()];
   __shared__ unsigned s_arrived;
   if (threadIdx.x == 0) s_arrived = 0u;
   __syncthreads();
   TW tw;
-  tw.init(g, blockIdx.x, offs);
+  const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
+  tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float C[NP][3], T[NP], Tl[NP], gC[NP][3], gA[NP];
   int lp[NP];
-  tw.forward(g, prims, atlas, idx, s_pi[tw.warp], C, T, Tl, lp);
+  tw.forward(g, prims, atlas, idx, s_pi[tw.lw], C, T, Tl, lp);
   const float inv = 1.f / (3.f * (float)g.H * (float)g.W);
   float lsum = 0.f;
 #pragma unroll
@@ -652,7 +668,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
     gA[p] = 0.f;
     gC[p][0] = gC[p][1] = gC[p][2] = 0.f;
     if (!tw.valid[p]) continue;
-    const size_t q = (size_t)tw.py(blockIdx.x, g, p) * g.W + tw.px(blockIdx.x, g, p);
+    const size_t q = (size_t)tw.py(tile, g, p) * g.W + tw.px(tile, g, p);
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
       const float bg = background ? background[3 * q + ch] : 0.f;
@@ -671,18 +687,18 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
     lsum += __shfl_xor_sync(kFull, lsum, 2);
     lsum += __shfl_xor_sync(kFull, lsum, 1);
     if (tw.lane == 0) {
-      s_loss[tw.warp] = lsum;
+      s_loss[tw.lw] = lsum;
       __threadfence_block();
-      if (atomicAdd(&s_arrived, 1u) == (unsigned)(TW::NW - 1)) {
+      if (atomicAdd(&s_arrived, 1u) == (unsigned)(kCtaWarps<TS>() - 1)) {
         __threadfence_block();
         const volatile float* sl = s_loss;
         double t = 0.0;
-        for (int w = 0; w < TW::NW; ++w) t += sl[w];
+        for (int w = 0; w < kCtaWarps<TS>(); ++w) t += sl[w];
         atomicAdd(loss_out, t * (double)inv);
       }
     }
   }
-  tw.backward(g, prims, atlas, idx, s_pi[tw.warp], gC, gA, Tl, lp, gacc);
+  tw.backward(g, prims, atlas, idx, s_pi[tw.lw], gC, gA, Tl, lp, gacc);
 }
 
 // ---------------------------------------------------------------------------
@@ -705,7 +721,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
 int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                    const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD><<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, color, alpha, T_last, last_pos))));
   DBMP_CHECK_LAUNCH("forward_kernel");
   return DBMP_OK;
@@ -714,7 +730,7 @@ int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* a
 int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  unsigned long long* cnt, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (count_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (count_kernel<TSV, KD><<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, cnt))));
   DBMP_CHECK_LAUNCH("count_kernel");
   return DBMP_OK;
@@ -724,7 +740,7 @@ int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* 
                     const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
                     const float* grad_alpha, double* gacc, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD><<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
                                                    grad_alpha, gacc))));
   DBMP_CHECK_LAUNCH("backward_kernel");
@@ -743,7 +759,7 @@ int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atl
                  const float* target, const float* background, float* out_image, double* gacc, double* loss,
                  const int* skip_flag, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (fused_kernel<TSV, KD><<<g.T, kThreadsOf<TSV>(), 0, st>>>(
+  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (fused_kernel<TSV, KD><<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                    g, prims, atlas, offs, idx, target, background, out_image,
                                                    gacc, loss, skip_flag))));
   DBMP_CHECK_LAUNCH("fused_kernel");
