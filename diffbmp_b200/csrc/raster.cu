@@ -295,15 +295,11 @@ struct TileWalker {
         float m[NP];
         if (toff != kSolid) {
           entry_coords_any<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf, live, s);
-          bool any[NP];
+#pragma unroll
+          for (int p = 0; p < NP; ++p) entry_fetch<KIND>(g, atlas, toff, s[p]);
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
-            any[p] = __any_sync(kFull, s[p].ok);
-            if (any[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
-          }
-#pragma unroll
-          for (int p = 0; p < NP; ++p) {
-            m[p] = any[p] ? blend<false>(s[p], nullptr, nullptr) : 0.f;
+            m[p] = blend<false>(s[p], nullptr, nullptr);
             if (STATS) {
               const bool c = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
               n_cand += c;
@@ -412,19 +408,12 @@ struct TileWalker {
         for (int p = 0; p < NP; ++p) live[p] = pos <= lp[p];
         Sample s[NP];
         float m[NP], gx[NP], gy[NP];
-        bool anyp[NP];
         if (toff != kSolid) {
           entry_coords_any<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf, live, s);
 #pragma unroll
-          for (int p = 0; p < NP; ++p) {
-            anyp[p] = __any_sync(kFull, s[p].ok);
-            if (anyp[p]) entry_fetch<KIND>(g, atlas, toff, s[p]);
-          }
+          for (int p = 0; p < NP; ++p) entry_fetch<KIND>(g, atlas, toff, s[p]);
 #pragma unroll
-          for (int p = 0; p < NP; ++p) {
-            m[p] = 0.f; gx[p] = gy[p] = 0.f;
-            if (anyp[p]) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
-          }
+          for (int p = 0; p < NP; ++p) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
         } else {
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
@@ -439,7 +428,6 @@ struct TileWalker {
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
           const bool frag = s[p].ok && m[p] > 1e-6f;
-          if (!__any_sync(kFull, frag)) continue;
           const float a = frag ? g2.x * m[p] : 0.f;
           const float om = fmaxf(1.f - a, 0.f);
           // T entering this fragment: stored for the last contributor, else
@@ -450,7 +438,9 @@ struct TileWalker {
           Ts[p] = Tk;
           const float gCc = fmaf(gC[p][0], g2.y, fmaf(gC[p][1], g2.z, gC[p][2] * g2.w));
           const float dLda = frag ? Tk * (gCc - H[p] + gA[p] * B[p]) : 0.f;
-          const float u = dLda * gx[p], v = dLda * gy[p];
+          // selects, not products with dLda = 0: the mask gradient of a pixel
+          // without a fragment comes from a redirected texel and may be NaN
+          const float u = frag ? dLda * gx[p] : 0.f, v = frag ? dLda * gy[p] : 0.f;
           const float ex = s[p].tx - g.hx, ey = s[p].ty - g.hy;
           acc[0] += u;
           acc[1] += v;
