@@ -6,10 +6,11 @@
 Workload (default): the precision-form configuration -- 2048x2048 canvas,
 N=20000 primitives drawn from a 16-bitmap 256x256 atlas, one image-fitting
 iteration per step (device binning + forward + L2 loss + backward + Adam).
-``value`` is iterations/s of the FP16-storage fused step, replayed from a
-CUDA graph with every input resident in HBM; the plain FP32 kernels
-(unfused forward / backward, FP32 atlas) are timed beside it on the same
-scene.  ``e2e`` is the same iteration through the public Python API with the
+``value`` is iterations/s of the FP16-storage fused step (half-precision
+bilinear-quad atlas), replayed from a CUDA graph with every input resident in
+HBM; the plain FP32 kernels (unfused forward / backward, FP32 atlas in the
+reference layout) and the FP16 pair-layout atlas are timed beside it on the
+same scene.  ``e2e`` is the same iteration through the public Python API with the
 primitive parameters uploaded from pinned host memory before each step and
 the loss read back after it.  Multi-GPU (torchrun): every rank fits its own
 independent job (replicas, no collective on the data path); value sums the
@@ -39,9 +40,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd iters/s at 2048^2 N=20k (FP16-storage fused vs plain FP32)"
-# DRAM bytes of one fused_kernel launch on the 2048^2 / N=20k scene, from one
-# ncu capture (read 106.9 MB + write 4.7 MB); null for other configs.
-FUSED_DRAM_BYTES_C2 = 111.586e6
+HEADLINE_KIND = "f16q"          # FP16 bilinear-quad atlas
+HEADLINE_KERNEL = "fused_kernel<32, F16_QUAD>"
+# DRAM bytes of one fused_kernel launch (FP16 quad atlas) on the 2048^2 / N=20k
+# scene, from one ncu capture (read 108.5 MB + write 3.8 MB); null for other configs.
+FUSED_DRAM_BYTES_C2 = 112.305e6
 
 
 def parse():
@@ -258,7 +261,8 @@ def run_serving(n_jobs, seed, torch):
     rate = 200.0
     reqs = serving.poisson_requests(n_jobs, rate, atlas, seed=seed, iterations=100, device="cuda")
     torch.cuda.synchronize()
-    srv = serving.Server(torch.from_numpy(atlas).cuda(), kind="f16", fused=True, max_slots=48, hbm_budget=150e9)
+    srv = serving.Server(torch.from_numpy(atlas).cuda(), kind=HEADLINE_KIND, fused=True, max_slots=48,
+                         hbm_budget=150e9)
     warm = serving.poisson_requests(2, rate, atlas, seed=seed + 999, iterations=5, sizes=(256,), device="cuda")
     srv.run(warm, realtime=False)
     res = srv.run(reqs, realtime=True)
@@ -331,7 +335,7 @@ def main():
         pass
 
     # --- headline: FP16-storage fused step, graph replayed ----------------
-    job = build_job(spec, "f16", True, torch)
+    job = build_job(spec, HEADLINE_KIND, True, torch)
     for _ in range(3):   # a timed region with a skipped (overflowed) step is discarded
         with ClockSampler(local) as clk:
             t_fused, replayed = time_steps(job, args.steps, args.warmup, torch, world)
@@ -348,9 +352,14 @@ def main():
     fused32 = build_job(spec, "f32", True, torch)
     t_fused32, _ = time_steps(fused32, args.steps, args.warmup, torch, world)
     t_fused32 = max_over_ranks(t_fused32, world)
+    del fused32
+    pair = build_job(spec, "f16", True, torch)
+    t_pair, _ = time_steps(pair, args.steps, args.warmup, torch, world)
+    t_pair = max_over_ranks(t_pair, world)
+    del pair
 
     # --- e2e through the public API with host buffers ---------------------
-    e2e_job = build_job(spec, "f16", True, torch)
+    e2e_job = build_job(spec, HEADLINE_KIND, True, torch)
     host = {k: torch.from_numpy(np.ascontiguousarray(getattr(spec, k), np.float32)).pin_memory()
             for k in ("means2D", "radii", "rotations", "opacities", "colors")}
     loss_host = torch.zeros(1, dtype=torch.float64).pin_memory()
@@ -398,21 +407,24 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.config}: {spec.H}x{spec.W} canvas, N={spec.N}, "
                                f"{spec.templates.shape[0]}x{spec.templates.shape[1]}x{spec.templates.shape[2]} atlas; "
-                               "one fit iteration per step (device binning, fused fwd+L2+bwd, Adam) with FP16-pair atlas "
+                               "one fit iteration per step (device binning, fused fwd+L2+bwd, Adam) with FP16 bilinear-quad atlas "
                                "storage and FP32 arithmetic, CUDA-graph replay",
                    "canvas": [spec.H, spec.W], "N": spec.N, "tile_size": 32, "t_stop": job.cfg.t_stop,
                    "l2": "per-step working set (target 50 MB + background 50 MB + tile lists 28 MB) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world}", "tile_list_entries": L, "replayed_steps": replayed},
         "plain_fp32": {"iters_per_s": world * args.steps / t_plain, "ms_per_step": t_plain / args.steps * 1e3,
                        "what": "unfused forward + torch L2 gradient + backward, FP32 atlas, graph replay"},
-        "fused_fp32": {"iters_per_s": world * args.steps / t_fused32, "ms_per_step": t_fused32 / args.steps * 1e3},
+        "fused_fp32": {"iters_per_s": world * args.steps / t_fused32, "ms_per_step": t_fused32 / args.steps * 1e3,
+                       "what": "fused kernel, FP32 atlas in the reference layout"},
+        "fused_f16_pair": {"iters_per_s": world * args.steps / t_pair, "ms_per_step": t_pair / args.steps * 1e3,
+                           "what": "fused kernel, FP16 atlas as horizontal texel pairs (half the FP32 bytes)"},
         "speedup_vs_plain_fp32": (world * args.steps / t_fused) / (world * args.steps / t_plain),
         "loss_after": loss_fused,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": FUSED_DRAM_BYTES,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                                       "kernel on this workload (profiles/fused_kernel_c2_f16pair.md)",
-                     "kernel": "fused_kernel<32, F16_PAIR>", "kernel_ms": t_kernel * 1e3,
+                                       "kernel on this workload (profiles/fused_kernel_c2_f16quad.md)",
+                     "kernel": HEADLINE_KERNEL, "kernel_ms": t_kernel * 1e3,
                      "flop_model": "12*C + 144*F_live (C pairs passing cull, F_live fragments composited)",
                      "C": cand, "F_live": frag, "warp_entries": went, "live_pixel_slots": slots,
                      "footprint_rejects": miss, "empty_warp_entries": empty, "grid_skips": clear,
