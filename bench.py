@@ -50,8 +50,8 @@ FUSED_DRAM_BYTES_C2 = 112.305e6
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c0", "c1", "c2"])
     ap.add_argument("--fast", action="store_true", help="skip the CPU-baseline leg")

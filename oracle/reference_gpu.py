@@ -10,6 +10,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 RASTER = os.path.join(_HERE, "_ref", "libref_raster.so")
 PSD = os.path.join(_HERE, "_ref", "libref_psd.so")
+RASTER16 = os.path.join(_HERE, "_ref", "libref_raster_fp16.so")
 
 
 def available() -> bool:
@@ -33,3 +34,16 @@ def psd():
     if _psd is None:
         _psd = ctypes.CDLL(PSD)
     return _psd
+
+
+_raster16 = None
+
+
+def raster_fp16():
+    """The reference's all-half kernels, or None when they are not built."""
+    global _raster16
+    if _raster16 is None and os.path.exists(RASTER16):
+        _raster16 = ctypes.CDLL(RASTER16)
+        _raster16.ref_forward_fp16.restype = ctypes.c_int
+        _raster16.ref_backward_fp16.restype = ctypes.c_int
+    return _raster16
