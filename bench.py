@@ -435,8 +435,8 @@ def main():
                 "d2h_bytes_per_step": 8,
                 "what": "public API: params H2D from pinned host, ImageFitter.step(), loss D2H, synchronised"},
         "gpu_launches": 6 * args.steps,
-        "gpu_launches_note": "ours per step: prepare, bin_rows<count>, bin_rows<write>, fused, adam, step_increment "
-                             "(+ the two kernels of one CUB exclusive scan over the tile counts)",
+        "gpu_launches_note": "ours per step: prepare, counts, bin_rows, fused, adam, step_increment "
+                             "(+ one memset and the two kernels of one CUB exclusive scan over the tile counts)",
         "clocks": clocks,
     }
     if args.serving_jobs > 0:

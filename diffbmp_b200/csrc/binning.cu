@@ -141,7 +141,7 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
                                const float* __restrict__ rot, const float* __restrict__ opac,
                                const float* __restrict__ colors, const int* __restrict__ sel,
                                const float* __restrict__ tbbox, int bin_mode, PrimInfo* __restrict__ out,
-                               int4* __restrict__ rects) {
+                               int4* __restrict__ rects, int* __restrict__ diff, int span) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= g.N) return;
   const float mx = means2D[2 * n], my = means2D[2 * n + 1];
@@ -208,18 +208,31 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
     }
   }
   rects[n] = make_int4(sx.x, sx.y, sy.x, sy.y);
+  if (diff != nullptr && sx.x <= sx.y && sy.x <= sy.y) {
+    // the rectangle's corners in its slice's 2-D difference array of
+    // (tilesY+1) x (tilesX+1) counters; its 2-D prefix sum is the number of
+    // the slice's rectangles covering each tile
+    const int gw = g.tilesX + 1;
+    int* d = diff + (size_t)(n / span) * (g.tilesY + 1) * gw;
+    atomicAdd(d + sy.x * gw + sx.x, 1);
+    atomicAdd(d + sy.x * gw + sx.y + 1, -1);
+    atomicAdd(d + (sy.y + 1) * gw + sx.x, -1);
+    atomicAdd(d + (sy.y + 1) * gw + sx.y + 1, 1);
+  }
 }
 
-// Tile lists, one CTA per (tile row, group of kBinGroup tiles, primitive
-// slice), one warp per tile.  The CTA walks the primitives of its slice in
-// index order in chunks of kBinThreads, compacts those whose rectangle covers
-// its row and overlaps its tile group, and each warp scans the compacted
-// chunk for rectangles containing its tile: with WRITE=false it counts them
-// into counts[t * S + slice]; with WRITE=true it writes their ids from
-// offs[t * S + slice] on.  The exclusive scan of the counts is tile-major and
-// slice-minor, so a tile's entries come out in ascending primitive order.
-// The WRITE pass also publishes tile_offsets, L and the overflow flag, and
-// leaves the outputs untouched when L exceeds the capacity.
+// Tile lists.  Counts: per primitive slice, prepare_kernel marks each
+// rectangle's corners in a 2-D difference array and counts_kernel prefix-sums
+// it into counts[t * S + slice], the number of the slice's rectangles covering
+// tile t.  The exclusive scan of the counts is tile-major and slice-minor.
+// Write: one CTA per (tile row, group of kBinGroup tiles, primitive slice),
+// one warp per tile; the CTA walks the primitives of its slice in index order
+// in chunks of kBinThreads, compacts those whose rectangle covers its row and
+// overlaps its tile group, and each warp writes the ids of the compacted
+// rectangles containing its tile from offs[t * S + slice] on, so a tile's
+// entries come out in ascending primitive order.  The write pass also
+// publishes tile_offsets, L and the overflow flag, and leaves the outputs
+// untouched when L exceeds the capacity.
 constexpr int kBinThreads = 512;
 constexpr int kBinGroup = kBinThreads / 32;
 
@@ -246,9 +259,28 @@ static inline BinGrid bin_grid(int N, int tilesX, int tilesY) {
   return b;
 }
 
-template <bool WRITE>
+// One CTA per slice: 2-D inclusive prefix sum of the slice's difference array
+// (rows, then columns), written as counts[t * S + slice]; counts[T * S] = 0.
+__global__ void counts_kernel(Geom g, BinGrid bg, int* __restrict__ diff, long long* __restrict__ counts) {
+  const int slice = blockIdx.x;
+  const int gw = g.tilesX + 1;
+  int* d = diff + (size_t)slice * (g.tilesY + 1) * gw;
+  for (int y = threadIdx.x; y < g.tilesY; y += blockDim.x) {
+    int acc = 0;
+    for (int x = 0; x < g.tilesX; ++x) { acc += d[y * gw + x]; d[y * gw + x] = acc; }
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < g.tilesX; x += blockDim.x) {
+    long long acc = 0;
+    for (int y = 0; y < g.tilesY; ++y) {
+      acc += d[y * gw + x];
+      counts[((long long)y * g.tilesX + x) * bg.slices + slice] = acc;
+    }
+  }
+  if (slice == 0 && threadIdx.x == 0) counts[(long long)g.T * bg.slices] = 0;
+}
+
 __global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid bg, const int4* __restrict__ rects,
-                                                               long long* __restrict__ counts,
                                                                const long long* __restrict__ offs, long long cap,
                                                                int* __restrict__ indices,
                                                                int* __restrict__ tile_offsets,
@@ -268,7 +300,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid b
   const long long nslots = (long long)g.T * bg.slices;
   const unsigned lt = (1u << lane) - 1u;
   long long cur = 0;
-  if (WRITE) {
+  {
     const long long L = offs[nslots];
     const bool first = blockIdx.x == 0 && threadIdx.x == 0;
     if (first) {
@@ -281,8 +313,6 @@ __global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid b
       cur = offs[slot];
       if (lane == 0 && slice == 0) tile_offsets[t] = (int)cur;
     }
-  } else if (blockIdx.x == 0 && threadIdx.x == 0) {
-    counts[nslots] = 0;
   }
   const int lo = slice * bg.span, hi = min(g.N, lo + bg.span);
   int4 rc = make_int4(1, 0, 1, 0);
@@ -312,14 +342,13 @@ __global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid b
       for (int j = lane; j < ((total + 31) & ~31); j += 32) {
         const bool in = j < total && s_x0[j] <= tx && tx <= s_x1[j];
         const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (WRITE && in) indices[cur + __popc(m & lt)] = s_id[j];
+        if (in) indices[cur + __popc(m & lt)] = s_id[j];
         cur += __popc(m);
       }
     }
     __syncthreads();   // the compacted chunk is reused by the next iteration
     rc = rn;
   }
-  if (!WRITE && has_tile && lane == 0) counts[slot] = cur;
 }
 
 // ---------------------------------------------------------------------------
@@ -327,6 +356,8 @@ struct BinWorkspace {
   int4* rects;         // N tile rectangles (x0, x1, y0, y1)
   long long* counts;   // T*S+1 entries per (tile, primitive slice)
   long long* offs;     // exclusive prefix of counts
+  int* diff;           // S difference arrays of (tilesY+1) x (tilesX+1)
+  size_t diff_bytes;
   void* cub_tmp;
   size_t cub_bytes;
   size_t total;
@@ -334,7 +365,8 @@ struct BinWorkspace {
 
 static inline size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
-static BinWorkspace layout_ws(void* base, int N, int T, long long nslots, bool query, size_t* needed) {
+static BinWorkspace layout_ws(void* base, int N, int T, long long nslots, size_t diff_bytes, bool query,
+                              size_t* needed) {
   BinWorkspace w{};
   size_t scan_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long*)nullptr, (long long*)nullptr, nslots + 1);
@@ -345,6 +377,8 @@ static BinWorkspace layout_ws(void* base, int N, int T, long long nslots, bool q
   const size_t o_counts = take(sizeof(long long) * (size_t)(nslots + 1));
   const size_t o_offs = take(sizeof(long long) * (size_t)(nslots + 1));
   const size_t o_cub = take(w.cub_bytes);
+  const size_t o_diff = take(diff_bytes);
+  w.diff_bytes = diff_bytes;
   w.total = off;
   if (needed) *needed = off;
   if (!query) {
@@ -353,15 +387,20 @@ static BinWorkspace layout_ws(void* base, int N, int T, long long nslots, bool q
     w.counts = reinterpret_cast<long long*>(b + o_counts);
     w.offs = reinterpret_cast<long long*>(b + o_offs);
     w.cub_tmp = b + o_cub;
+    w.diff = reinterpret_cast<int*>(b + o_diff);
   }
   return w;
+}
+
+static inline size_t diff_bytes_of(const BinGrid& bg, int tilesX, int tilesY) {
+  return sizeof(int) * (size_t)bg.slices * (tilesY + 1) * (tilesX + 1);
 }
 
 size_t bin_workspace_bytes(int N, int T, int tilesX, int tilesY, long long cap) {
   (void)cap;   // the row binning needs no scratch per list entry
   const BinGrid bg = bin_grid(N, tilesX, tilesY);
   size_t need = 0;
-  layout_ws(nullptr, N, T, (long long)T * bg.slices, true, &need);
+  layout_ws(nullptr, N, T, (long long)T * bg.slices, diff_bytes_of(bg, tilesX, tilesY), true, &need);
   return need;
 }
 
@@ -448,7 +487,7 @@ int launch_prepare(const Geom& g, const float* means2D, const float* radii, cons
                    const float* colors, const int* sel, PrimInfo* out, cudaStream_t st) {
   if (g.N == 0) return DBMP_OK;
   prepare_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(g, means2D, radii, rot, opac, colors, sel, nullptr, 0,
-                                                    out, nullptr);
+                                                    out, nullptr, nullptr, 1);
   DBMP_CHECK_LAUNCH("prepare_kernel");
   return DBMP_OK;
 }
@@ -460,27 +499,28 @@ int launch_bin(const Geom& g, int bin_mode, const float* means2D, const float* r
   const BinGrid bg = bin_grid(g.N, g.tilesX, g.tilesY);
   const long long nslots = (long long)g.T * bg.slices;
   size_t need = 0;
-  BinWorkspace w = layout_ws(ws, g.N, g.T, nslots, false, &need);
+  BinWorkspace w = layout_ws(ws, g.N, g.T, nslots, diff_bytes_of(bg, g.tilesX, g.tilesY), false, &need);
   if (ws_bytes < need) {
     set_error("dbmp_bin: workspace of %zu bytes is smaller than the %zu bytes required", ws_bytes, need);
     return DBMP_ERR_CAPACITY;
   }
+  if (bg.ctas > 0x7fffffffll) { set_error("dbmp_bin: canvas and primitive count too large"); return DBMP_ERR_INVALID; }
+  cudaError_t e = cudaMemsetAsync(w.diff, 0, w.diff_bytes, st);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(diff)");
   if (g.N > 0) {
     prepare_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(g, means2D, radii, rot, opac, colors, sel, tbbox, bin_mode,
-                                                      prim_info, w.rects);
+                                                      prim_info, w.rects, w.diff, bg.span);
     DBMP_CHECK_LAUNCH("prepare_kernel");
   }
-  if (bg.ctas > 0x7fffffffll) { set_error("dbmp_bin: canvas and primitive count too large"); return DBMP_ERR_INVALID; }
-  const int grid = (int)bg.ctas;   // (tile row, tile group, primitive slice) triples
-  bin_rows_kernel<false><<<grid, kBinThreads, 0, st>>>(g, bg, w.rects, w.counts, nullptr, cap, nullptr, nullptr,
-                                                       nullptr, nullptr);
-  DBMP_CHECK_LAUNCH("bin_rows_kernel<count>");
+  counts_kernel<<<bg.slices, 1024, 0, st>>>(g, bg, w.diff, w.counts);
+  DBMP_CHECK_LAUNCH("counts_kernel");
   size_t tmp = w.cub_bytes;
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(w.cub_tmp, tmp, w.counts, w.offs, nslots + 1, st);
+  e = cub::DeviceScan::ExclusiveSum(w.cub_tmp, tmp, w.counts, w.offs, nslots + 1, st);
   if (e != cudaSuccess) return cuda_status(e, "cub::DeviceScan::ExclusiveSum");
-  bin_rows_kernel<true><<<grid, kBinThreads, 0, st>>>(g, bg, w.rects, nullptr, w.offs, cap, tile_indices,
-                                                      tile_offsets, total_out, overflow_out);
-  DBMP_CHECK_LAUNCH("bin_rows_kernel<write>");
+  const int grid = (int)bg.ctas;   // (tile row, tile group, primitive slice) triples
+  bin_rows_kernel<<<grid, kBinThreads, 0, st>>>(g, bg, w.rects, w.offs, cap, tile_indices, tile_offsets, total_out,
+                                                overflow_out);
+  DBMP_CHECK_LAUNCH("bin_rows_kernel");
   return DBMP_OK;
 }
 

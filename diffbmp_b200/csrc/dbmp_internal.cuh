@@ -65,7 +65,10 @@ __host__ __device__ inline int template_records(int kind, int Ht, int Wt) {
 // records, 256-byte aligned.
 constexpr int kGridCap = 64;
 constexpr float kGridSupport = 5e-7f;
-constexpr int kGridMaxCells = 64;   // cells per axis at most
+#ifndef DBMP_GRID_CELLS
+#define DBMP_GRID_CELLS 128
+#endif
+constexpr int kGridMaxCells = DBMP_GRID_CELLS;   // cells per axis at most
 
 __host__ __device__ inline void grid_shape(int n, int* shift, int* cells) {
   int s = 0;

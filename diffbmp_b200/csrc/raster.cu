@@ -94,25 +94,36 @@ __device__ __forceinline__ void entry_coords(const Geom& g, const float4& g0, co
   }
 }
 
-template <int NP, class L>
-__device__ __forceinline__ void entry_coords_any(const Geom& g, const float4& g0, const float4& g1, bool inside,
-                                                 bool fast, const float (&pxf)[NP], const float (&pyf)[NP],
-                                                 const bool (&live)[NP], Sample (&s)[NP]) {
-  if (fast) entry_coords<NP, L, true>(g, g0, g1, inside, pxf, pyf, live, s);
-  else entry_coords<NP, L, false>(g, g0, g1, inside, pxf, pyf, live, s);
-}
-
 // Phase 2 for one pixel: sampling position and texel fetch (texel 0 of the
 // template when the pixel cannot yield a fragment, so the load is in bounds).
-template <int KIND>
+template <int KIND, bool FAST>
 __device__ __forceinline__ void entry_fetch(const Geom& g, const void* __restrict__ atlas, int toff, Sample& s) {
-  const float tx = s.ok ? s.tx : 0.f, ty = s.ok ? s.ty : 0.f;
+  // FAST: every pixel's coordinate lies inside the template, no redirection needed
+  const float tx = (FAST || s.ok) ? s.tx : 0.f, ty = (FAST || s.ok) ? s.ty : 0.f;
   float fx, fy;
   const int x0 = floor_small(tx, &fx);
   const int y0 = floor_small(ty, &fy);
   s.wx = tx - fx;
   s.wy = ty - fy;
   s.q = AtlasFetch<KIND>::get(atlas, toff, g.Ht, g.Wt, x0, y0);
+}
+
+// Texel coordinates and texel fetches of all pixels of the thread for one
+// entry (fast: the entry's warp-uniform interior bit).
+template <int NP, class L, int KIND>
+__device__ __forceinline__ void entry_sample(const Geom& g, const void* __restrict__ atlas, int toff,
+                                             const float4& g0, const float4& g1, bool inside, bool fast,
+                                             const float (&pxf)[NP], const float (&pyf)[NP],
+                                             const bool (&live)[NP], Sample (&s)[NP]) {
+  if (fast) {
+    entry_coords<NP, L, true>(g, g0, g1, inside, pxf, pyf, live, s);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) entry_fetch<KIND, true>(g, atlas, toff, s[p]);
+  } else {
+    entry_coords<NP, L, false>(g, g0, g1, inside, pxf, pyf, live, s);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) entry_fetch<KIND, false>(g, atlas, toff, s[p]);
+  }
 }
 
 // Bilinear mask (clamped) and, with GRAD, its texel-space gradient.
@@ -294,9 +305,8 @@ struct TileWalker {
         Sample s[NP];
         float m[NP];
         if (toff != kSolid) {
-          entry_coords_any<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf, live, s);
-#pragma unroll
-          for (int p = 0; p < NP; ++p) entry_fetch<KIND>(g, atlas, toff, s[p]);
+          entry_sample<NP, L, KIND>(g, atlas, toff, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf,
+                                    live, s);
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
             m[p] = blend<false>(s[p], nullptr, nullptr);
@@ -334,7 +344,7 @@ struct TileWalker {
           C[p][2] = fmaf(wt, g2.w, C[p][2]);
           Tl[p] = frag ? T[p] : Tl[p];
           lp[p] = frag ? pos : lp[p];
-          T[p] *= fmaxf(1.f - a, 0.f);
+          T[p] = fmaxf(fmaf(-T[p], a, T[p]), 0.f);   // T (1 - a), 0 when a > 1 (alpha_max > 1)
           live[p] = live[p] && !(T[p] < g.t_stop);
           local_done = local_done && !live[p];
         }
@@ -409,9 +419,8 @@ struct TileWalker {
         Sample s[NP];
         float m[NP], gx[NP], gy[NP];
         if (toff != kSolid) {
-          entry_coords_any<NP, L>(g, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf, live, s);
-#pragma unroll
-          for (int p = 0; p < NP; ++p) entry_fetch<KIND>(g, atlas, toff, s[p]);
+          entry_sample<NP, L, KIND>(g, atlas, toff, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf,
+                                    live, s);
 #pragma unroll
           for (int p = 0; p < NP; ++p) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
         } else {
@@ -437,10 +446,11 @@ struct TileWalker {
           const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
           Ts[p] = Tk;
           const float gCc = fmaf(gC[p][0], g2.y, fmaf(gC[p][1], g2.z, gC[p][2] * g2.w));
-          const float dLda = frag ? Tk * (gCc - H[p] + gA[p] * B[p]) : 0.f;
-          // selects, not products with dLda = 0: the mask gradient of a pixel
-          // without a fragment comes from a redirected texel and may be NaN
-          const float u = frag ? dLda * gx[p] : 0.f, v = frag ? dLda * gy[p] : 0.f;
+          // a pixel without a fragment contributes nothing: a = 0 zeroes its colour
+          // and opacity terms, and its mask gradient (from a redirected texel,
+          // possibly NaN) is replaced by 0 rather than multiplied by 0
+          const float dLda = Tk * (gCc - H[p] + gA[p] * B[p]);
+          const float u = dLda * (frag ? gx[p] : 0.f), v = dLda * (frag ? gy[p] : 0.f);
           const float ex = s[p].tx - g.hx, ey = s[p].ty - g.hy;
           acc[0] += u;
           acc[1] += v;

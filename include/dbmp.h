@@ -83,7 +83,7 @@ int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* o
  *   row y = Ht; out holds P*(Ht+1)*Wt*2 elements.
  * Neighbours outside the template are 0.  The texel records are followed,
  * at the next 256-byte boundary, by a clearance grid: per template, cells of
- * 2^s x 2^t texels (s, t the smallest shifts giving at most 64 cells per
+ * 2^s x 2^t texels (s, t the smallest shifts giving at most 128 cells per
  * axis), one byte each, the L-infinity distance in texels (capped at 64) from
  * the cell to the nearest texel > 5e-7 or NaN.  The tile walk uses it to skip
  * warp footprints where a primitive's mask cannot pass the fragment test

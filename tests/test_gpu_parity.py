@@ -215,7 +215,7 @@ def test_precision_forms_gpu(kind, min_psnr):
 
 # ---------------------------------------------------------------------------
 # clearance grid of the packed atlases
-def _grid_bruteforce(t, cap=64, max_cells=64):
+def _grid_bruteforce(t, cap=64, max_cells=128):
     """Per cell: min over support texels (> 5e-7 or NaN) of the L-infinity
     distance from the cell's coordinate range to the texel, capped (the
     definition, evaluated directly)."""
