@@ -96,16 +96,22 @@ __host__ __device__ inline size_t atlas_grid_offset(int P, int Ht, int Wt, int k
 
 // Thread layout of the tile walk: one CTA per TS x TS tile, NP pixels per
 // thread, each warp owning an FW x FH footprint.
+// DBMP_SQUARE_FOOTPRINT: with 2 pixels per thread, an 8x8 warp footprint
+// (the second pixel 4 rows below the first) instead of 16x4.
+#ifndef DBMP_SQUARE_FOOTPRINT
+#define DBMP_SQUARE_FOOTPRINT 1
+#endif
 template <int TS, int NP>
 struct Layout {
   static_assert(NP == 1 || NP == 2 || NP == 4, "pixels per thread");
-  static constexpr int FW = NP >= 2 ? 16 : 8;     // warp footprint
-  static constexpr int FH = NP == 4 ? 8 : 4;
+  static constexpr bool kSq = DBMP_SQUARE_FOOTPRINT && NP == 2;
+  static constexpr int FW = kSq ? 8 : (NP >= 2 ? 16 : 8);     // warp footprint
+  static constexpr int FH = kSq ? 8 : (NP == 4 ? 8 : 4);
   static constexpr int WPR = TS / FW;              // warps per footprint row
   static constexpr int NW = (TS / FW) * (TS / FH);
   static constexpr int NT = NW * 32;
-  static __device__ __forceinline__ int ox(int p) { return 8 * (p & 1); }
-  static __device__ __forceinline__ int oy(int p) { return 4 * (p >> 1); }
+  static __host__ __device__ __forceinline__ int ox(int p) { return kSq ? 0 : 8 * (p & 1); }
+  static __host__ __device__ __forceinline__ int oy(int p) { return kSq ? 4 * p : 4 * (p >> 1); }
 };
 
 // Pixels per thread of each tile size (tuned on B200).
