@@ -261,13 +261,38 @@ static inline BinGrid bin_grid(int N, int tilesX, int tilesY) {
 
 // One CTA per slice: 2-D inclusive prefix sum of the slice's difference array
 // (rows, then columns), written as counts[t * S + slice]; counts[T * S] = 0.
-__global__ void counts_kernel(Geom g, BinGrid bg, int* __restrict__ diff, long long* __restrict__ counts) {
+// SMEM: the array is staged in shared memory (it fits for canvases up to
+// about 3500 x 3500 pixels at tile 32); otherwise it is scanned in place.
+// Rows are scanned by whole warps (shuffle scans over 32-column chunks),
+// columns by one thread each.
+template <bool SMEM>
+__global__ void __launch_bounds__(1024) counts_kernel(Geom g, BinGrid bg, int* __restrict__ diff,
+                                                      long long* __restrict__ counts) {
+  extern __shared__ int s_diff[];
   const int slice = blockIdx.x;
   const int gw = g.tilesX + 1;
-  int* d = diff + (size_t)slice * (g.tilesY + 1) * gw;
-  for (int y = threadIdx.x; y < g.tilesY; y += blockDim.x) {
-    int acc = 0;
-    for (int x = 0; x < g.tilesX; ++x) { acc += d[y * gw + x]; d[y * gw + x] = acc; }
+  const int cells = (g.tilesY + 1) * gw;
+  int* src = diff + (size_t)slice * cells;
+  int* d = SMEM ? s_diff : src;
+  if (SMEM) {
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) s_diff[i] = src[i];
+    __syncthreads();
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int y = warp; y < g.tilesY; y += nwarps) {
+    int carry = 0;
+    for (int x0 = 0; x0 < g.tilesX; x0 += 32) {
+      const int x = x0 + lane;
+      int v = x < g.tilesX ? d[y * gw + x] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      v += carry;
+      if (x < g.tilesX) d[y * gw + x] = v;
+      carry = __shfl_sync(0xffffffffu, v, 31);
+    }
   }
   __syncthreads();
   for (int x = threadIdx.x; x < g.tilesX; x += blockDim.x) {
@@ -512,7 +537,9 @@ int launch_bin(const Geom& g, int bin_mode, const float* means2D, const float* r
                                                       prim_info, w.rects, w.diff, bg.span);
     DBMP_CHECK_LAUNCH("prepare_kernel");
   }
-  counts_kernel<<<bg.slices, 1024, 0, st>>>(g, bg, w.diff, w.counts);
+  const size_t cells_bytes = sizeof(int) * (size_t)(g.tilesY + 1) * (g.tilesX + 1);
+  if (cells_bytes <= 48 * 1024) counts_kernel<true><<<bg.slices, 1024, cells_bytes, st>>>(g, bg, w.diff, w.counts);
+  else counts_kernel<false><<<bg.slices, 1024, 0, st>>>(g, bg, w.diff, w.counts);
   DBMP_CHECK_LAUNCH("counts_kernel");
   size_t tmp = w.cub_bytes;
   e = cub::DeviceScan::ExclusiveSum(w.cub_tmp, tmp, w.counts, w.offs, nslots + 1, st);
