@@ -54,6 +54,8 @@ SIGNATURES = {
     "dbmp_backward": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                            _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_backward_noalloc": (_i, [_CP] + [_vp] * 18),
+    "dbmp_forward_blend": (_i, [_CP] + [_vp] * 5 + [_f] + [_vp] * 5),
+    "dbmp_backward_blend": (_i, [_CP] + [_vp] * 5 + [_f] + [_vp] * 15),
     "dbmp_backward_noalloc_max_prims": (_i, []),
     "dbmp_psd_bboxes": (_i, [_vp, _vp, _i, _i, _i, _f, _vp, _vp, _vp]),
     "dbmp_psd_layout": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),

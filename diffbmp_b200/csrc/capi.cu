@@ -34,6 +34,12 @@ int launch_bin(const Geom& g, int bin_mode, const float* means2D, const float* r
                void* ws, size_t ws_bytes, cudaStream_t st);
 int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                    const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st);
+int launch_forward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                         const int* idx, float* color, float* alpha, float* T_last, int* last_pos, const float* cmap,
+                         float cblend, cudaStream_t st);
+int launch_backward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                          const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
+                          const float* grad_alpha, double* gacc, const float* cmap, float cblend, cudaStream_t st);
 int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  unsigned long long* cnt, cudaStream_t st);
 int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
@@ -213,6 +219,49 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
   }
   rc = launch_backward(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices, T_last,
                        last_pos, grad_color, grad_alpha, grad_accum, st);
+  if (rc) return rc;
+  return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
+                         grad_rotations, grad_opacities, grad_colors, st);
+}
+
+int dbmp_forward_blend(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
+                       const int32_t* tile_indices, const float* colors_orig, float c_blend, float* out_color,
+                       float* out_alpha, float* T_last, int32_t* last_pos, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_forward_blend");
+  if (rc) return rc;
+  REQUIRE(atlas && tile_offsets && tile_indices && out_color && out_alpha && T_last && last_pos,
+          "dbmp_forward_blend: null pointer");
+  REQUIRE(g.N == 0 || prim_info, "dbmp_forward_blend: prim_info is null");
+  REQUIRE(c_blend >= 0.f && c_blend <= 1.f, "dbmp_forward_blend: c_blend %g outside [0, 1]", (double)c_blend);
+  REQUIRE(c_blend == 0.f || g.N == 0 || colors_orig, "dbmp_forward_blend: colors_orig is null with c_blend > 0");
+  return launch_forward_blend(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices,
+                              out_color, out_alpha, T_last, last_pos, colors_orig, c_blend, (cudaStream_t)stream);
+}
+
+int dbmp_backward_blend(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
+                        const int32_t* tile_indices, const float* colors_orig, float c_blend, const float* T_last,
+                        const int32_t* last_pos, const float* grad_color, const float* grad_alpha,
+                        const float* radii, const float* rotations, const float* opacities, const float* colors,
+                        double* grad_accum, float* grad_means2D, float* grad_radii, float* grad_rotations,
+                        float* grad_opacities, float* grad_colors, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_backward_blend");
+  if (rc) return rc;
+  REQUIRE(atlas && tile_offsets && tile_indices && T_last && last_pos && grad_color,
+          "dbmp_backward_blend: null input");
+  REQUIRE(g.N == 0 || (prim_info && radii && rotations && opacities && colors), "dbmp_backward_blend: null parameter");
+  REQUIRE(g.N == 0 || (grad_accum && grad_means2D && grad_radii && grad_rotations && grad_opacities && grad_colors),
+          "dbmp_backward_blend: null output");
+  REQUIRE(c_blend >= 0.f && c_blend <= 1.f, "dbmp_backward_blend: c_blend %g outside [0, 1]", (double)c_blend);
+  REQUIRE(c_blend == 0.f || g.N == 0 || colors_orig, "dbmp_backward_blend: colors_orig is null with c_blend > 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (g.N > 0) {
+    cudaError_t e = cudaMemsetAsync(grad_accum, 0, sizeof(double) * 8 * (size_t)g.N, st);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(grad_accum)");
+  }
+  rc = launch_backward_blend(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices,
+                             T_last, last_pos, grad_color, grad_alpha, grad_accum, colors_orig, c_blend, st);
   if (rc) return rc;
   return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
                          grad_rotations, grad_opacities, grad_colors, st);

@@ -140,6 +140,29 @@ __device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
   return fmaxf(0.f, fminf(1.f, m));
 }
 
+// Colour-map sample (tile_forward.cu:17-89): the texel coordinate is clamped
+// into the map, neighbours past the last row / column repeat it, bilinear in
+// the reference's operation order.  cm: the primitive's (Ht,Wt,3) map.
+__device__ __forceinline__ float3 sample_cmap(const float* __restrict__ cm, int Ht, int Wt, float tx, float ty) {
+  const float cx = fmaxf(0.f, fminf((float)(Wt - 1), tx));
+  const float cy = fmaxf(0.f, fminf((float)(Ht - 1), ty));
+  const int x0 = (int)cx, y0 = (int)cy;
+  const int x1 = min(x0 + 1, Wt - 1), y1 = min(y0 + 1, Ht - 1);
+  const float fx = cx - (float)x0, fy = cy - (float)y0;
+  const float* p00 = cm + 3 * (y0 * Wt + x0);
+  const float* p10 = cm + 3 * (y0 * Wt + x1);
+  const float* p01 = cm + 3 * (y1 * Wt + x0);
+  const float* p11 = cm + 3 * (y1 * Wt + x1);
+  float r[3];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    const float c0 = __ldg(p00 + ch) * (1.f - fx) + __ldg(p10 + ch) * fx;
+    const float c1 = __ldg(p01 + ch) * (1.f - fx) + __ldg(p11 + ch) * fx;
+    r[ch] = c0 * (1.f - fy) + c1 * fy;
+  }
+  return make_float3(r[0], r[1], r[2]);
+}
+
 // ---------------------------------------------------------------------------
 // Ballots of one staged chunk (bit j = entry base + j).
 struct ChunkMasks {
@@ -150,7 +173,9 @@ struct ChunkMasks {
   unsigned miss;     // footprint misses the cull square
 };
 
-template <int TS, int NP, int KIND>
+// CB: fragment colours blend a per-primitive colour map (cmap, (N,Ht,Wt,3))
+// with weight cblend, (1 - cblend) sigmoid(c) + cblend c_o (tile_forward.cu:316-330).
+template <int TS, int NP, int KIND, bool CB = false>
 struct TileWalker {
   using L = Layout<TS, NP>;
   static constexpr int NT = L::NT;
@@ -158,6 +183,16 @@ struct TileWalker {
   static constexpr bool kGrid = KIND != ATLAS_F32;   // packed atlases carry a clearance grid
 
   int warp, lw, lane, start, end;   // warp: index within the tile, lw: within the CTA
+  const float* cmap = nullptr;
+  float cblend = 0.f;
+
+  // Fragment colour of pixel sample s for primitive id (g2.yzw = sigmoid(c)).
+  __device__ __forceinline__ float3 frag_colour(const Geom& g, const float4& g2, int id, const Sample& s) const {
+    if (!CB) return make_float3(g2.y, g2.z, g2.w);
+    const float3 co = sample_cmap(cmap + (size_t)id * g.Ht * g.Wt * 3, g.Ht, g.Wt, s.tx, s.ty);
+    const float k = 1.f - cblend;
+    return make_float3(k * g2.y + cblend * co.x, k * g2.z + cblend * co.y, k * g2.w + cblend * co.z);
+  }
   float pxf[NP], pyf[NP];
   bool valid[NP];
   float fx0, fx1, fy0, fy1, fcx, fcy;
@@ -339,9 +374,16 @@ struct TileWalker {
           if (STATS) { n_frag += frag; n_depth[p] += frag; }
           const float a = frag ? g2.x * m[p] : 0.f;
           const float wt = T[p] * a;
-          C[p][0] = fmaf(wt, g2.y, C[p][0]);
-          C[p][1] = fmaf(wt, g2.z, C[p][1]);
-          C[p][2] = fmaf(wt, g2.w, C[p][2]);
+          if (CB) {
+            const float3 col = frag_colour(g, g2, __shfl_sync(kFull, my_id, e), s[p]);
+            C[p][0] = fmaf(wt, col.x, C[p][0]);
+            C[p][1] = fmaf(wt, col.y, C[p][1]);
+            C[p][2] = fmaf(wt, col.z, C[p][2]);
+          } else {
+            C[p][0] = fmaf(wt, g2.y, C[p][0]);
+            C[p][1] = fmaf(wt, g2.z, C[p][1]);
+            C[p][2] = fmaf(wt, g2.w, C[p][2]);
+          }
           Tl[p] = frag ? T[p] : Tl[p];
           lp[p] = frag ? pos : lp[p];
           T[p] = fmaxf(fmaf(-T[p], a, T[p]), 0.f);   // T (1 - a), 0 when a > 1 (alpha_max > 1)
@@ -445,7 +487,8 @@ struct TileWalker {
           // Ts is unchanged when there is no fragment).
           const float Tk = (pos == lp[p]) ? Ts[p] : __fdividef(Ts[p], om);
           Ts[p] = Tk;
-          const float gCc = fmaf(gC[p][0], g2.y, fmaf(gC[p][1], g2.z, gC[p][2] * g2.w));
+          const float3 col = frag_colour(g, g2, id, s[p]);
+          const float gCc = fmaf(gC[p][0], col.x, fmaf(gC[p][1], col.y, gC[p][2] * col.z));
           // a pixel without a fragment contributes nothing: a = 0 zeroes its colour
           // and opacity terms, and its mask gradient (from a redirected texel,
           // possibly NaN) is replaced by 0 rather than multiplied by 0
@@ -516,15 +559,17 @@ template <int TS> constexpr int kBlocksPerSM() {
 }
 
 // ---------------------------------------------------------------------------
-template <int TS, int KIND>
+template <int TS, int KIND, bool CB>
 __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) forward_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, float* __restrict__ out_color, float* __restrict__ out_alpha,
-    float* __restrict__ T_last, int* __restrict__ last_pos) {
+    float* __restrict__ T_last, int* __restrict__ last_pos, const float* __restrict__ cmap, float cblend) {
   constexpr int NP = DefaultNP<TS>::v;
-  using TW = TileWalker<TS, NP, KIND>;
+  using TW = TileWalker<TS, NP, KIND, CB>;
   __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
   TW tw;
+  tw.cmap = cmap;
+  tw.cblend = cblend;
   const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
   tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float C[NP][3], T[NP], Tl[NP];
@@ -563,15 +608,18 @@ __global__ void __launch_bounds__(kThreadsOf<TS>()) count_kernel(Geom g, const P
   if (threadIdx.x == 0 && part == 0) atomicAdd(cnt + 2, (unsigned long long)(tw.end - tw.start));
 }
 
-template <int TS, int KIND>
+template <int TS, int KIND, bool CB>
 __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, const float* __restrict__ T_last, const int* __restrict__ last_pos,
-    const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc) {
+    const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc,
+    const float* __restrict__ cmap, float cblend) {
   constexpr int NP = DefaultNP<TS>::v;
-  using TW = TileWalker<TS, NP, KIND>;
+  using TW = TileWalker<TS, NP, KIND, CB>;
   __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
   TW tw;
+  tw.cmap = cmap;
+  tw.cblend = cblend;
   const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
   tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float gC[NP][3], gA[NP], Ts[NP];
@@ -718,13 +766,28 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
   else if ((ts) == 16) { constexpr int TSV = 16; __VA_ARGS__; }      \
   else { set_error("tile_size %d is not supported (16 or 32)", ts); return DBMP_ERR_INVALID; }
 
-int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
-                   const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st) {
+int launch_forward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                         const int* idx, float* color, float* alpha, float* T_last, int* last_pos, const float* cmap,
+                         float cblend, cudaStream_t st) {
   if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD><<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
-                                                   g, prims, atlas, offs, idx, color, alpha, T_last, last_pos))));
+  if (cmap != nullptr && cblend > 0.f) {
+    DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD, true>
+                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                     g, prims, atlas, offs, idx, color, alpha, T_last, last_pos,
+                                                     cmap, cblend))));
+  } else {
+    DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD, false>
+                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                     g, prims, atlas, offs, idx, color, alpha, T_last, last_pos,
+                                                     nullptr, 0.f))));
+  }
   DBMP_CHECK_LAUNCH("forward_kernel");
   return DBMP_OK;
+}
+
+int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                   const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st) {
+  return launch_forward_blend(g, kind, prims, atlas, offs, idx, color, alpha, T_last, last_pos, nullptr, 0.f, st);
 }
 
 int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
@@ -736,15 +799,30 @@ int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atl
   return DBMP_OK;
 }
 
+int launch_backward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
+                          const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
+                          const float* grad_alpha, double* gacc, const float* cmap, float cblend, cudaStream_t st) {
+  if (g.T == 0) return DBMP_OK;
+  if (cmap != nullptr && cblend > 0.f) {
+    DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD, true>
+                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                     g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
+                                                     grad_alpha, gacc, cmap, cblend))));
+  } else {
+    DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD, false>
+                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                     g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
+                                                     grad_alpha, gacc, nullptr, 0.f))));
+  }
+  DBMP_CHECK_LAUNCH("backward_kernel");
+  return DBMP_OK;
+}
+
 int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                     const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
                     const float* grad_alpha, double* gacc, cudaStream_t st) {
-  if (g.T == 0) return DBMP_OK;
-  DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD><<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
-                                                   g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
-                                                   grad_alpha, gacc))));
-  DBMP_CHECK_LAUNCH("backward_kernel");
-  return DBMP_OK;
+  return launch_backward_blend(g, kind, prims, atlas, offs, idx, T_last, last_pos, grad_color, grad_alpha, gacc,
+                               nullptr, 0.f, st);
 }
 
 int launch_finalize(const Geom& g, const float* radii, const float* rot, const float* opac, const float* colors,

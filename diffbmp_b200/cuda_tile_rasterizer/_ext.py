@@ -58,11 +58,6 @@ def _get(fp16):
     return g
 
 
-def _check_blend(c_blend, colors_orig):
-    if colors_orig is not None and colors_orig.numel() > 0 and float(c_blend) > 0.0:
-        raise NotImplementedError("c_blend > 0 (per-pixel colour-map blending) is not supported by this build")
-
-
 def _f(t):
     return t.detach().to(torch.float32).contiguous()
 
@@ -70,7 +65,6 @@ def _f(t):
 def forward(fp16, means2D, radii, rotations, opacities, colors, colors_orig, templates, sel, c_blend, mapping,
             keep=True):
     g = _get(fp16)
-    _check_blend(c_blend, colors_orig)
     t0 = time.perf_counter()
     atlas = g.get_atlas(templates)
     m, r, th, v, c = _f(means2D).view(-1, 2), _f(radii).view(-1), _f(rotations).view(-1), _f(opacities).view(-1), \
@@ -78,7 +72,11 @@ def forward(fp16, means2D, radii, rotations, opacities, colors, colors_orig, tem
     s = sel.to(torch.int32).contiguous().view(-1)
     has_map = mapping is not None and isinstance(mapping, torch.Tensor) and mapping.numel() > 0
     rz = g.rz_map if has_map else g.rz_cull
-    color, alpha, state = rz.forward(m, r, th, v, c, s, atlas, mapping if has_map else None)
+    # colour-map blending (tile_forward.cu:316-330) when colors_orig is given and c_blend > 0
+    blend = colors_orig is not None and isinstance(colors_orig, torch.Tensor) and colors_orig.numel() > 0 \
+        and float(c_blend) > 0.0
+    color, alpha, state = rz.forward(m, r, th, v, c, s, atlas, mapping if has_map else None, None,
+                                     _f(colors_orig) if blend else None, float(c_blend) if blend else 0.0)
     if keep:
         g.states = [(state, rz, atlas)]
     g.t_fwd += (time.perf_counter() - t0) * 1e3

@@ -95,6 +95,8 @@ class ForwardState:
     lists: TileLists
     T_last: torch.Tensor
     last_pos: torch.Tensor
+    colors_orig: Optional[torch.Tensor] = None   # colour maps of a blended render
+    c_blend: float = 0.0
 
 
 def lists_from_mapping(mapping: torch.Tensor, num_tiles: int, num_prims: int) -> TileLists:
@@ -189,10 +191,14 @@ class Rasterizer:
 
     # -- forward / backward -------------------------------------------------
     def forward(self, means2D, radii, rotations, opacities, colors, sel, atlas: Atlas,
-                mapping: Optional[torch.Tensor] = None, stream=None):
-        """Returns (color (H,W,3), alpha (H,W), ForwardState)."""
+                mapping: Optional[torch.Tensor] = None, stream=None, colors_orig: Optional[torch.Tensor] = None,
+                c_blend: float = 0.0):
+        """Returns (color (H,W,3), alpha (H,W), ForwardState).  With
+        colors_orig (N,Ht,Wt,3) and c_blend in (0, 1], fragment colours blend
+        the per-primitive colour maps (dbmp_forward_blend)."""
         _need_cuda(means2D, radii, rotations, opacities, colors, sel)
         N = int(radii.shape[0])
+        cmap = self._colour_maps(colors_orig, c_blend, N, atlas)
         if mapping is not None and mapping.numel() > 0:
             lists = lists_from_mapping(mapping, self.T, N)
             prim_info = self.prepare(means2D, radii, rotations, opacities, colors, sel, atlas, stream)
@@ -203,9 +209,28 @@ class Rasterizer:
         alpha = torch.empty((self.H, self.W), dtype=torch.float32, device=self.device)
         T_last = torch.empty((self.H, self.W), dtype=torch.float32, device=self.device)
         last_pos = torch.empty((self.H, self.W), dtype=torch.int32, device=self.device)
-        call("dbmp_forward", ctypes.byref(cv), _ptr(prim_info), _ptr(atlas.data), _ptr(lists.offsets),
-             _ptr(lists.indices), _ptr(color), _ptr(alpha), _ptr(T_last), _ptr(last_pos), _stream(stream))
-        return color, alpha, ForwardState(prim_info, lists, T_last, last_pos)
+        if cmap is None:
+            call("dbmp_forward", ctypes.byref(cv), _ptr(prim_info), _ptr(atlas.data), _ptr(lists.offsets),
+                 _ptr(lists.indices), _ptr(color), _ptr(alpha), _ptr(T_last), _ptr(last_pos), _stream(stream))
+            return color, alpha, ForwardState(prim_info, lists, T_last, last_pos)
+        call("dbmp_forward_blend", ctypes.byref(cv), _ptr(prim_info), _ptr(atlas.data), _ptr(lists.offsets),
+             _ptr(lists.indices), _ptr(cmap), ctypes.c_float(c_blend), _ptr(color), _ptr(alpha), _ptr(T_last),
+             _ptr(last_pos), _stream(stream))
+        return color, alpha, ForwardState(prim_info, lists, T_last, last_pos, cmap, float(c_blend))
+
+    @staticmethod
+    def _colour_maps(colors_orig, c_blend, N, atlas: Atlas):
+        """The (N,Ht,Wt,3) f32 colour maps of a blended render, or None."""
+        if colors_orig is None or colors_orig.numel() == 0 or float(c_blend) <= 0.0:
+            return None
+        if not 0.0 < float(c_blend) <= 1.0:
+            raise ValueError(f"c_blend {c_blend} outside [0, 1]")
+        _need_cuda(colors_orig)
+        cm = _f32(colors_orig)
+        if cm.numel() != N * atlas.Ht * atlas.Wt * 3:
+            raise ValueError(f"colors_orig has {cm.numel()} values, expected N*Ht*Wt*3 = "
+                             f"{N}*{atlas.Ht}*{atlas.Wt}*3")
+        return cm
 
     def backward(self, state: ForwardState, grad_color, grad_alpha, radii, rotations, opacities, colors,
                  atlas: Atlas, stream=None):
@@ -222,10 +247,17 @@ class Rasterizer:
         g_rot = torch.empty(N, dtype=torch.float32, device=dev)
         g_op = torch.empty(N, dtype=torch.float32, device=dev)
         g_col = torch.empty((N, 3), dtype=torch.float32, device=dev)
-        call("dbmp_backward", ctypes.byref(cv), _ptr(state.prim_info), _ptr(atlas.data),
-             _ptr(state.lists.offsets), _ptr(state.lists.indices), _ptr(state.T_last), _ptr(state.last_pos),
-             _ptr(gc), _ptr(ga), _ptr(radii), _ptr(rotations), _ptr(opacities), _ptr(colors), _ptr(acc),
-             _ptr(g_means), _ptr(g_r), _ptr(g_rot), _ptr(g_op), _ptr(g_col), _stream(stream))
+        if state.colors_orig is None:
+            call("dbmp_backward", ctypes.byref(cv), _ptr(state.prim_info), _ptr(atlas.data),
+                 _ptr(state.lists.offsets), _ptr(state.lists.indices), _ptr(state.T_last), _ptr(state.last_pos),
+                 _ptr(gc), _ptr(ga), _ptr(radii), _ptr(rotations), _ptr(opacities), _ptr(colors), _ptr(acc),
+                 _ptr(g_means), _ptr(g_r), _ptr(g_rot), _ptr(g_op), _ptr(g_col), _stream(stream))
+        else:
+            call("dbmp_backward_blend", ctypes.byref(cv), _ptr(state.prim_info), _ptr(atlas.data),
+                 _ptr(state.lists.offsets), _ptr(state.lists.indices), _ptr(state.colors_orig),
+                 ctypes.c_float(state.c_blend), _ptr(state.T_last), _ptr(state.last_pos),
+                 _ptr(gc), _ptr(ga), _ptr(radii), _ptr(rotations), _ptr(opacities), _ptr(colors), _ptr(acc),
+                 _ptr(g_means), _ptr(g_r), _ptr(g_rot), _ptr(g_op), _ptr(g_col), _stream(stream))
         return g_means, g_r, g_rot, g_op, g_col
 
 
@@ -233,17 +265,22 @@ class RasterizeFunction(torch.autograd.Function):
     """Differentiable render of bitmap primitives (hand-written backward).
 
     forward(means2D (N,2), radii (N), rotations (N), opacities (N), colors (N,3),
-            sel (N) int, atlas, rasterizer, mapping) -> (color (H,W,3), alpha (H,W))
+            sel (N) int, atlas, rasterizer, mapping, colors_orig, c_blend)
+        -> (color (H,W,3), alpha (H,W))
     Gradients flow to the five parameter tensors, as in the reference's
-    TileRasterizerFunction (cuda_tile_rasterizer/__init__.py:254-340).
+    TileRasterizerFunction (cuda_tile_rasterizer/__init__.py:254-340); the
+    colour maps colors_orig get none, as there.
     """
 
     @staticmethod
-    def forward(ctx, means2D, radii, rotations, opacities, colors, sel, atlas, rasterizer, mapping=None):
+    def forward(ctx, means2D, radii, rotations, opacities, colors, sel, atlas, rasterizer, mapping=None,
+                colors_orig=None, c_blend=0.0):
         m, r, th, v, c = (_f32(t) for t in (means2D, radii, rotations, opacities, colors))
         s = sel.detach().to(torch.int32).contiguous()
         color, alpha, state = rasterizer.forward(m.view(-1, 2), r.view(-1), th.view(-1), v.view(-1),
-                                                 c.view(-1, 3), s.view(-1), atlas, mapping)
+                                                 c.view(-1, 3), s.view(-1), atlas, mapping, None,
+                                                 None if colors_orig is None else colors_orig.detach(),
+                                                 float(c_blend))
         ctx.state = state
         ctx.atlas = atlas
         ctx.rasterizer = rasterizer
@@ -261,9 +298,11 @@ class RasterizeFunction(torch.autograd.Function):
                                           c.view(-1, 3), ctx.atlas)
         sh = ctx.shapes
         return (gm.view(sh[0]), gr.view(sh[1]), gth.view(sh[2]), gv.view(sh[3]), gc.view(sh[4]),
-                None, None, None, None)
+                None, None, None, None, None, None)
 
 
 def rasterize(means2D, radii, rotations, opacities, colors, sel, atlas: Atlas, rasterizer: Rasterizer,
-              mapping: Optional[torch.Tensor] = None):
-    return RasterizeFunction.apply(means2D, radii, rotations, opacities, colors, sel, atlas, rasterizer, mapping)
+              mapping: Optional[torch.Tensor] = None, colors_orig: Optional[torch.Tensor] = None,
+              c_blend: float = 0.0):
+    return RasterizeFunction.apply(means2D, radii, rotations, opacities, colors, sel, atlas, rasterizer, mapping,
+                                   colors_orig, c_blend)

@@ -180,6 +180,31 @@ int dbmp_backward_noalloc(const dbmp_canvas* cv, const void* prim_info, const vo
 /* Largest N dbmp_backward_noalloc accepts. */
 int dbmp_backward_noalloc_max_prims(void);
 
+/* Forward / backward with colour-map blending (c_blend > 0): each fragment's
+ * colour is (1 - c_blend) sigmoid(c) + c_blend c_o, where c_o is the
+ * primitive's colour map colors_orig (N,Ht,Wt,3) f32 in [0,1] sampled at the
+ * fragment's texel coordinate, clamped into the map and bilinear with
+ * edge-repeating neighbours.  Replaces the colors_orig / c_blend branch of
+ * tile_rasterize_forward_kernel (cuda_tile_rasterizer/cuda_kernels/
+ * tile_forward.cu:17-89,316-330) and its backward (tile_backward.cu:228-270):
+ * dL/dalpha uses the blended colour; the colour-logit gradient is
+ * gC alpha T sigma'(c) without a (1 - c_blend) factor and the colour map's
+ * dependence on the geometry is not differentiated, as in the reference.
+ * c_blend = 0 or colors_orig = NULL is dbmp_forward / dbmp_backward.
+ * c_blend must lie in [0, 1]. */
+int dbmp_forward_blend(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+                       const int32_t* tile_offsets, const int32_t* tile_indices,
+                       const float* colors_orig, float c_blend, float* out_color, float* out_alpha,
+                       float* T_last, int32_t* last_pos, void* stream);
+int dbmp_backward_blend(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
+                        const int32_t* tile_offsets, const int32_t* tile_indices,
+                        const float* colors_orig, float c_blend, const float* T_last,
+                        const int32_t* last_pos, const float* grad_color, const float* grad_alpha,
+                        const float* radii, const float* rotations, const float* opacities,
+                        const float* colors, double* grad_accum, float* grad_means2D,
+                        float* grad_radii, float* grad_rotations, float* grad_opacities,
+                        float* grad_colors, void* stream);
+
 /* Counting pass over the same walk as dbmp_forward (no image output):
  * counts[0] = (pixel, primitive) pairs that pass the square cull before the
  * pixel terminates, counts[1] = fragments composited, counts[2] = tile-list

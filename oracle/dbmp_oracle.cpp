@@ -57,6 +57,8 @@ struct Scene {
   double edge;            // boundary shift: > 0 widens the cull and the texel cut
                           // by `edge` (pixels / texels), < 0 narrows them; tests
                           // use +-edge renders to find boundary-sensitive pixels
+  const double* cmap = nullptr;   // (N,Ht,Wt,3) colour maps (colors_orig), or null
+  double cblend = 0.0;            // colour-map blend weight (used when cmap && cblend > 0)
 };
 
 inline double sigmoid_d(double x) {
@@ -99,10 +101,28 @@ inline double sample_tmpl(const double* t, int Ht, int Wt, double x, double y,
   return f;
 }
 
+// Colour map sample at texel coordinate (x, y), tile_forward.cu:17-89: the
+// coordinate is clamped into the map, neighbours past the last row / column
+// repeat it (not zero), bilinear weights.
+inline void sample_cmap(const double* cm, int Ht, int Wt, double x, double y, double out[3]) {
+  const double cx = std::max(0.0, std::min((double)(Wt - 1), x));
+  const double cy = std::max(0.0, std::min((double)(Ht - 1), y));
+  const int x0 = (int)cx, y0 = (int)cy;
+  const int x1 = std::min(x0 + 1, Wt - 1), y1 = std::min(y0 + 1, Ht - 1);
+  const double fx = cx - x0, fy = cy - y0;
+  for (int ch = 0; ch < 3; ++ch) {
+    const double c00 = cm[3 * ((size_t)y0 * Wt + x0) + ch], c10 = cm[3 * ((size_t)y0 * Wt + x1) + ch];
+    const double c01 = cm[3 * ((size_t)y1 * Wt + x0) + ch], c11 = cm[3 * ((size_t)y1 * Wt + x1) + ch];
+    const double c0 = c00 * (1 - fx) + c10 * fx, c1 = c01 * (1 - fx) + c11 * fx;
+    out[ch] = c0 * (1 - fy) + c1 * fy;
+  }
+}
+
 struct Frag {
   int n;            // primitive id
   double a;         // alpha
-  double c[3];      // colour in [0,1]
+  double c[3];      // colour in [0,1] (blended with the colour map when enabled)
+  double sc[3];     // sigmoid of the colour logits
   double m;         // mask
   double gx, gy;    // d mask / d texel coordinate
   double ex, ey;    // texel coordinate minus template half extent
@@ -152,7 +172,13 @@ inline bool eval_pair(const Scene& s, int n, int px, int py, Frag* f, bool* cull
   f->n = n;
   f->m = m;
   f->a = s.amax * sop * m;
-  for (int ch = 0; ch < 3; ++ch) f->c[ch] = sigmoid_d(s.colors[3 * n + ch]);
+  for (int ch = 0; ch < 3; ++ch) f->sc[ch] = f->c[ch] = sigmoid_d(s.colors[3 * n + ch]);
+  if (s.sem == SEM_KERNEL && s.cmap != nullptr && s.cblend > 0.0) {
+    // tile_forward.cu:316-330: (1 - c_blend) sigmoid(c) + c_blend c_o(x, y)
+    double co[3];
+    sample_cmap(s.cmap + (size_t)n * s.Ht * s.Wt * 3, s.Ht, s.Wt, tx, ty, co);
+    for (int ch = 0; ch < 3; ++ch) f->c[ch] = (1.0 - s.cblend) * f->sc[ch] + s.cblend * co[ch];
+  }
   f->gx = gx; f->gy = gy;
   f->ex = tx - hx; f->ey = ty - hy;
   f->u = u; f->v = v; f->cs = cs; f->sn = sn; f->rinv = rinv; f->sop = sop;
@@ -355,13 +381,15 @@ long long orc_bin(int H, int W, int ts, const float* means2D, const float* radii
 // the transmittance entering the last contributor and its list position;
 // stats[0..4] = candidates (pairs passing the cull), fragments, live
 // fragments (walked before termination), max depth, list entries walked.
-int orc_forward(int H, int W, int ts, int N, const double* means2D, const double* radii, const double* rot,
-                const double* opac, const double* colors, int P, int Ht, int Wt, const double* tmpl,
-                const int* sel, double amax, int sem, double t_stop, double edge,
-                const int* offsets, const int* indices,
-                double* out_color, double* out_alpha, double* T_last, int* last_pos, long long* stats,
-                int nthreads) {
+int orc_forward_cmap(int H, int W, int ts, int N, const double* means2D, const double* radii, const double* rot,
+                     const double* opac, const double* colors, int P, int Ht, int Wt, const double* tmpl,
+                     const int* sel, double amax, int sem, double t_stop, double edge,
+                     const int* offsets, const int* indices,
+                     double* out_color, double* out_alpha, double* T_last, int* last_pos, long long* stats,
+                     int nthreads, const double* cmap, double cblend) {
   Scene s{H, W, ts, N, P, Ht, Wt, means2D, radii, rot, opac, colors, tmpl, sel, amax, sem, t_stop, edge};
+  s.cmap = cmap;
+  s.cblend = cblend;
   const int tX = tiles_x(s);
   const int nt = resolve_threads(nthreads, H);
   std::vector<long long> wc(nt, 0), wf(nt, 0), wl(nt, 0);
@@ -397,12 +425,15 @@ int orc_forward(int H, int W, int ts, int N, const double* means2D, const double
 // SEM_KERNEL follows tile_backward.cu:212-343 literally (suffix S, back
 // product B, 1/max(1-a,1e-6)); SEM_TORCH is the exact derivative of the
 // torch composite (autograd through cumprod / grid_sample).
-int orc_backward(int H, int W, int ts, int N, const double* means2D, const double* radii, const double* rot,
-                 const double* opac, const double* colors, int P, int Ht, int Wt, const double* tmpl,
-                 const int* sel, double amax, int sem, double t_stop, double edge,
-                 const int* offsets, const int* indices,
-                 const float* grad_color, const float* grad_alpha, double* grads, int nthreads) {
+int orc_backward_cmap(int H, int W, int ts, int N, const double* means2D, const double* radii, const double* rot,
+                      const double* opac, const double* colors, int P, int Ht, int Wt, const double* tmpl,
+                      const int* sel, double amax, int sem, double t_stop, double edge,
+                      const int* offsets, const int* indices,
+                      const float* grad_color, const float* grad_alpha, double* grads, int nthreads,
+                      const double* cmap, double cblend) {
   Scene s{H, W, ts, N, P, Ht, Wt, means2D, radii, rot, opac, colors, tmpl, sel, amax, sem, t_stop, edge};
+  s.cmap = cmap;
+  s.cblend = cblend;
   const int tX = tiles_x(s);
   const double hx = 0.5 * (Wt - 1), hy = 0.5 * (Ht - 1);
   const int nt = resolve_threads(nthreads, H);
@@ -441,7 +472,10 @@ int orc_backward(int H, int W, int ts, int N, const double* means2D, const doubl
           dLda += gA * B;
           dLda *= f.T;
         }
-        for (int ch = 0; ch < 3; ++ch) gn[5 + ch] += gC[ch] * f.a * f.T * f.c[ch] * (1.0 - f.c[ch]);
+        // colour logits: gC a T sigma'(c), without a (1 - c_blend) factor, as
+        // the reference computes it (tile_backward.cu:254-262); the colour
+        // map's dependence on the geometry is not differentiated there either
+        for (int ch = 0; ch < 3; ++ch) gn[5 + ch] += gC[ch] * f.a * f.T * f.sc[ch] * (1.0 - f.sc[ch]);
         const double sop = f.sop;
         gn[4] += dLda * amax * f.m * sop * (1.0 - sop);
         const double dLdm = dLda * amax * sop;
@@ -469,6 +503,26 @@ int orc_backward(int H, int W, int ts, int N, const double* means2D, const doubl
 }
 
 // PSD stage 1 (psd_export_kernels.cu:12-55), float32 arithmetic.
+int orc_forward(int H, int W, int ts, int N, const double* means2D, const double* radii, const double* rot,
+                const double* opac, const double* colors, int P, int Ht, int Wt, const double* tmpl,
+                const int* sel, double amax, int sem, double t_stop, double edge,
+                const int* offsets, const int* indices,
+                double* out_color, double* out_alpha, double* T_last, int* last_pos, long long* stats,
+                int nthreads) {
+  return orc_forward_cmap(H, W, ts, N, means2D, radii, rot, opac, colors, P, Ht, Wt, tmpl, sel, amax, sem, t_stop,
+                          edge, offsets, indices, out_color, out_alpha, T_last, last_pos, stats, nthreads, nullptr,
+                          0.0);
+}
+
+int orc_backward(int H, int W, int ts, int N, const double* means2D, const double* radii, const double* rot,
+                 const double* opac, const double* colors, int P, int Ht, int Wt, const double* tmpl,
+                 const int* sel, double amax, int sem, double t_stop, double edge,
+                 const int* offsets, const int* indices,
+                 const float* grad_color, const float* grad_alpha, double* grads, int nthreads) {
+  return orc_backward_cmap(H, W, ts, N, means2D, radii, rot, opac, colors, P, Ht, Wt, tmpl, sel, amax, sem, t_stop,
+                           edge, offsets, indices, grad_color, grad_alpha, grads, nthreads, nullptr, 0.0);
+}
+
 int orc_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale,
                    int* bbox, int* sizes) {
   for (int n = 0; n < N; ++n) {

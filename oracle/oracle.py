@@ -115,7 +115,7 @@ class Scene:
     """Inputs of one render, as the reference extension receives them."""
 
     def __init__(self, H, W, ts, means2D, radii, rot, opac, colors, templates, sel,
-                 alpha_max=1.0):
+                 alpha_max=1.0, colors_orig=None, c_blend=0.0):
         self.H, self.W, self.ts = int(H), int(W), int(ts)
         # parameters are kept in float64: the kernels' float32 inputs convert
         # exactly, and finite-difference checks can perturb them below 1 ulp(f32)
@@ -128,6 +128,14 @@ class Scene:
         self.templates = t[None] if t.ndim == 2 else t
         self.sel = _i32(sel).reshape(-1)
         self.alpha_max = float(alpha_max)
+        # per-primitive colour maps (N,Ht,Wt,3) in [0,1] and their blend weight
+        # (tile_forward.cu:316-330); used when both are given and c_blend > 0
+        self.colors_orig = None if colors_orig is None else _f64(colors_orig)
+        self.c_blend = float(c_blend)
+
+    def _cmap_args(self):
+        use = self.colors_orig is not None and self.c_blend > 0
+        return (_p(self.colors_orig) if use else None, ctypes.c_double(self.c_blend if use else 0.0))
 
     @property
     def N(self):
@@ -152,9 +160,9 @@ def forward(scene: Scene, offs, idx, sem=SEM_KERNEL, t_stop=0.0, nthreads=0, edg
     tl = np.zeros((H, W), np.float64)
     lp = np.zeros((H, W), np.int32)
     stats = np.zeros(5, np.int64)
-    lib().orc_forward(*scene._args(), int(sem), ctypes.c_double(t_stop), ctypes.c_double(edge),
-                      _p(offs), _p(idx),
-                      _p(color), _p(alpha), _p(tl), _p(lp), _p(stats), int(nthreads))
+    lib().orc_forward_cmap(*scene._args(), int(sem), ctypes.c_double(t_stop), ctypes.c_double(edge),
+                           _p(offs), _p(idx),
+                           _p(color), _p(alpha), _p(tl), _p(lp), _p(stats), int(nthreads), *scene._cmap_args())
     return dict(color=color, alpha=alpha, T_last=tl, last_pos=lp,
                 stats=dict(candidates=int(stats[0]), fragments=int(stats[1]),
                            live=int(stats[2]), max_depth=int(stats[3])))
@@ -170,9 +178,9 @@ def backward(scene: Scene, offs, idx, grad_color, grad_alpha, sem=SEM_KERNEL, t_
     gc = _f32(grad_color).reshape(scene.H, scene.W, 3)
     ga = None if grad_alpha is None else _f32(grad_alpha).reshape(scene.H, scene.W)
     g = np.zeros((scene.N, 8), np.float64)
-    lib().orc_backward(*scene._args(), int(sem), ctypes.c_double(t_stop), ctypes.c_double(edge),
-                       _p(offs), _p(idx),
-                       _p(gc), _p(ga), _p(g), int(nthreads))
+    lib().orc_backward_cmap(*scene._args(), int(sem), ctypes.c_double(t_stop), ctypes.c_double(edge),
+                            _p(offs), _p(idx),
+                            _p(gc), _p(ga), _p(g), int(nthreads), *scene._cmap_args())
     return g
 
 

@@ -23,22 +23,26 @@ def cuda(a, dt=torch.float32):
     return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dt)
 
 
-@pytest.mark.parametrize("with_mapping", [True, False])
-def test_tile_rasterizer_call_matches_oracle(with_mapping):
+@pytest.mark.parametrize("with_mapping,c_blend", [(True, 0.0), (False, 0.0), (True, 0.3)])
+def test_tile_rasterizer_call_matches_oracle(with_mapping, c_blend):
+    """c_blend > 0 blends the colour maps colors_orig (tile_forward.cu:316-330)."""
     import diffbmp_b200.cuda_tile_rasterizer as ctr
     s, sel = scene(1)
     ts = 32
     sc = O.Scene(s.H, s.W, ts, s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.templates, sel)
+    co_np = np.random.default_rng(5).uniform(0, 1, (s.N, s.templates.shape[1], s.templates.shape[2], 3))
+    if c_blend > 0:
+        sc.colors_orig, sc.c_blend = co_np, c_blend
     offs, idx = bin_scene(sc, O.BIN_CONTENT if with_mapping else O.BIN_CULL)
     tr = ctr.TileRasterizer(s.H, s.W, ts, 0.0, 1.0, 400, s.N)
     x, y = cuda(s.means2D[:, 0]).requires_grad_(), cuda(s.means2D[:, 1]).requires_grad_()
     r, th = cuda(s.radii).requires_grad_(), cuda(s.rotations).requires_grad_()
     v, c = cuda(s.opacities).requires_grad_(), cuda(s.colors).requires_grad_()
-    co = torch.zeros((s.N, s.templates.shape[1], s.templates.shape[2], 3), device="cuda")
+    co = cuda(co_np)
     lr = torch.tensor([0.1, 1, 1, 1, 1, 1, 1.0], device="cuda")
     mapping = cuda(O.mapping_tensor(offs, idx), torch.int32) if with_mapping else None
-    color, alpha = tr(torch.stack([x, y], 1), r, th, v, c, co, cuda(s.templates), cuda(sel, torch.int64), 0.0, lr,
-                      mapping)
+    color, alpha = tr(torch.stack([x, y], 1), r, th, v, c, co, cuda(s.templates), cuda(sel, torch.int64), c_blend,
+                      lr, mapping)
     ref = O.forward(sc, offs, idx)
     band, _ = O.boundary_band(sc, offs, idx)
     err = np.abs(color.detach().cpu().numpy() - ref["color"]).max(-1)

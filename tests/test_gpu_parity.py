@@ -289,3 +289,45 @@ def test_clearance_grid_never_skips_a_fragment_gpu(name, kind, t_stop):
     assert c[8] <= c[7]
     if name == "atlas128":        # random shapes leave empty cells (the c0 soft disk has none)
         assert c[8] > 0
+
+
+# ---------------------------------------------------------------------------
+# colour-map blending (c_blend > 0)
+@pytest.mark.parametrize("name", ["c0", "atlas128", "ragged16", "nonsquare"])
+def test_colour_map_blend_parity_gpu(name):
+    """dbmp_forward_blend / dbmp_backward_blend against the FP64 oracle with
+    the reference's blend semantics, at the FP32 bars."""
+    sc = SCENES[name]()
+    rng = np.random.default_rng(11)
+    P, Ht, Wt = sc.templates.shape
+    cm = rng.uniform(0, 1, (sc.N, Ht, Wt, 3)).astype(np.float32)
+    sc.colors_orig, sc.c_blend = cm.astype(np.float64), 0.35
+    offs, idx = bin_scene(sc)
+    d = dev(sc)
+    rz = R.Rasterizer(sc.H, sc.W, sc.ts, sc.alpha_max, 1e-7)
+    atlas = R.Atlas(d["templates"])
+    tcm = torch.from_numpy(cm).cuda()
+    color, alpha, state = rz.forward(d["means2D"], d["radii"], d["rotations"], d["opacities"], d["colors"],
+                                     d["sel"], atlas, None, None, tcm, 0.35)
+    torch.cuda.synchronize()
+    r = check_image(sc, offs, idx, color.cpu().numpy(), alpha.cpu().numpy())
+    print(name, "image", r["max_err"])
+    gc = rng.normal(0, 1, (sc.H, sc.W, 3)).astype(np.float32)
+    ga = rng.normal(0, 1, (sc.H, sc.W)).astype(np.float32)
+    grads = rz.backward(state, torch.from_numpy(gc).cuda(), torch.from_numpy(ga).cuda(), d["radii"],
+                        d["rotations"], d["opacities"], d["colors"], atlas)
+    ours = np.concatenate([g.cpu().numpy().reshape(sc.N, -1) for g in grads], 1)
+    check_grads(sc, offs, idx, gc, ga, ours)
+    # the blend changes the image: c_blend = 0 renders something else
+    c0, *_ = rz.forward(d["means2D"], d["radii"], d["rotations"], d["opacities"], d["colors"], d["sel"], atlas)
+    assert (c0 - color).abs().max().item() > 1e-3
+
+
+def test_colour_map_blend_rejects_bad_input_gpu():
+    sc = SCENES["c0"]()
+    d = dev(sc)
+    rz = R.Rasterizer(sc.H, sc.W, sc.ts)
+    atlas = R.Atlas(d["templates"])
+    with pytest.raises(ValueError):
+        rz.forward(d["means2D"], d["radii"], d["rotations"], d["opacities"], d["colors"], d["sel"], atlas,
+                   None, None, torch.zeros(3, device="cuda"), 0.5)

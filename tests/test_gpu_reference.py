@@ -183,3 +183,66 @@ def test_forward_backward_vs_reference_kernels(name, ts):
         spread = np.linalg.norm(hi[:, k] - lo[:, k]) / nrm
         print(f"  block {k}: reference {e_r:.2e}, ours {e_o:.2e}, ours vs reference {e_ro:.2e}, band {spread:.2e}")
         assert e_ro <= max(1e-4, 2 * e_r) + spread
+
+
+def test_colour_map_blend_vs_reference_kernel():
+    """c_blend > 0: forward and backward against the reference's own kernels
+    with colour maps (tile_forward.cu:316-330, tile_backward.cu:228-270)."""
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.rasterizer import Atlas, Rasterizer
+    s = wl.make_scene("c0", 4)
+    sc = O.Scene(s.H, s.W, 32, s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.templates, s.sel)
+    P, Ht, Wt = sc.templates.shape
+    N, H, W = sc.N, sc.H, sc.W
+    rng = np.random.default_rng(8)
+    cm = rng.uniform(0, 1, (N, Ht, Wt, 3)).astype(np.float32)
+    cb = 0.35
+    sc.colors_orig, sc.c_blend = cm.astype(np.float64), cb
+    offs, idx = bin_scene(sc)
+    f = O.forward(sc, offs, idx)
+    K = f["stats"]["max_depth"] + 16
+    caches = torch.zeros(5 * H * W * K + 8 * K, dtype=torch.float32, device="cuda")
+    counts = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+    sig = torch.zeros(8 * N + 8, dtype=torch.float32, device="cuda")
+    d = dict(m=dev(sc.means2D), r=dev(sc.radii), th=dev(sc.rot), v=dev(sc.opac), c=dev(sc.colors),
+             t=dev(sc.templates), s=dev(sc.sel, np.int32), o=dev(offs, np.int32), i=dev(np.maximum(idx, 0), np.int32))
+    tcm = dev(cm)
+    rcol = torch.zeros((H, W, 3), device="cuda")
+    ralp = torch.zeros((H, W), device="cuda")
+    Lr = RG.raster()
+    rc = Lr.ref_forward_cb(H, W, 32, ctypes.c_float(1.0), N, P, Ht, Wt, K, P_(d["m"]), P_(d["r"]), P_(d["th"]),
+                           P_(d["v"]), P_(d["c"]), P_(tcm), ctypes.c_float(cb), P_(d["t"]), P_(d["s"]), P_(d["o"]),
+                           len(offs), P_(d["i"]), len(idx), P_(rcol), P_(ralp), P_(caches), P_(counts), P_(sig))
+    assert rc == 0
+    rz = Rasterizer(H, W, 32, t_stop=1e-7)
+    atlas = Atlas(d["t"])
+    col, alp, state = rz.forward(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], atlas, None, None, tcm, cb)
+    torch.cuda.synchronize()
+    e_ref = np.abs(rcol.cpu().numpy() - f["color"]).max()
+    band, _ = O.boundary_band(sc, offs, idx, edge=1e-3)
+    diff = np.abs(col.cpu().numpy() - rcol.cpu().numpy()).max(-1)
+    print(f"blend: reference vs FP64 {e_ref:.2e}; ours vs reference outside band {diff[band == 0].max(initial=0):.2e}")
+    assert diff[band == 0].max(initial=0) <= max(2e-5, 2 * e_ref)
+
+    gc = rng.normal(0, 1, (H, W, 3)).astype(np.float32)
+    ga = rng.normal(0, 1, (H, W)).astype(np.float32)
+    t_gc, t_ga = dev(gc), dev(ga)
+    rg = [torch.zeros(sh, device="cuda") for sh in ((N, 2), (N,), (N,), (N,), (N, 3))]
+    rc = Lr.ref_backward_cb(H, W, 32, ctypes.c_float(1.0), N, P, Ht, Wt, K, P_(d["m"]), P_(d["r"]), P_(d["th"]),
+                            P_(d["v"]), P_(d["c"]), P_(tcm), ctypes.c_float(cb), P_(d["t"]), P_(d["s"]), P_(d["o"]),
+                            len(offs), P_(d["i"]), len(idx), P_(t_gc), P_(t_ga), P_(caches), P_(counts), P_(sig),
+                            *[P_(t) for t in rg])
+    assert rc == 0
+    ours = rz.backward(state, t_gc, t_ga, d["r"], d["th"], d["v"], d["c"], atlas)
+    refo = O.backward(sc, offs, idx, gc, ga)
+    hi = O.backward(sc, offs, idx, gc, ga, edge=1e-3)
+    lo = O.backward(sc, offs, idx, gc, ga, edge=-1e-3)
+    rgn = np.concatenate([t.cpu().numpy().reshape(N, -1) for t in rg], 1)
+    ogn = np.concatenate([t.cpu().numpy().reshape(N, -1) for t in ours], 1)
+    for k in range(8):
+        nrm = np.linalg.norm(refo[:, k])
+        e_r = np.linalg.norm(rgn[:, k] - refo[:, k]) / nrm
+        e_ro = np.linalg.norm(ogn[:, k] - rgn[:, k]) / nrm
+        spread = np.linalg.norm(hi[:, k] - lo[:, k]) / nrm
+        print(f"  block {k}: reference vs FP64 {e_r:.2e}, ours vs reference {e_ro:.2e}, band {spread:.2e}")
+        assert e_ro <= max(1e-4, 2 * e_r) + spread

@@ -92,6 +92,33 @@ def test_kat_full_occlusion():
     assert f["alpha"][20, 22] == 1.0
 
 
+def test_kat_colour_map_blend():
+    """c_blend > 0 (tile_forward.cu:316-330): colour = (1-cb) sigmoid(c) + cb c_o, with
+    c_o the colour map sampled at the texel coordinate (clamped, edge-repeating);
+    the colour-logit gradient is gC a T sigma'(c) without (1-cb), as the
+    reference computes it (tile_backward.cu:254-262)."""
+    Ht = Wt = 9
+    cm = np.zeros((1, Ht, Wt, 3))
+    cm[..., 0] = np.linspace(0, 1, Wt)[None, :]           # red ramps with the texel column
+    cm[..., 1] = 0.25
+    cm[..., 2] = np.linspace(1, 0, Ht)[:, None]           # blue ramps down the rows
+    sc = _one_prim_scene(np.ones((Ht, Wt), np.float32), 20.0, 20.0, 4.0, v=0.3)
+    sc.colors_orig, sc.c_blend = cm, 0.4
+    f = _render(sc)
+    a, cb, sc_ = sig(0.3), 0.4, sig([0.2, -0.4, 1.1])
+    # pixel (x=22, y=19): texel (x, y) = ((2/4)+1)*4, ((-1/4)+1)*4 = (6, 3)
+    co = np.array([6 / 8, 0.25, 1 - 3 / 8])
+    assert np.allclose(f["color"][19, 22], a * ((1 - cb) * sc_ + cb * co), atol=1e-14)
+    offs, idx = bin_scene(sc, O.BIN_CULL)
+    gc = np.zeros((40, 48, 3), np.float32)
+    gc[19, 22] = (1.0, 2.0, -1.0)
+    g = O.backward(sc, offs, idx, gc, None)
+    assert np.allclose(g[0, 5:8], np.array([1.0, 2.0, -1.0]) * a * sc_ * (1 - sc_), atol=1e-14)
+    # the opacity gradient sees the blended colour
+    assert g[0, 4] == pytest.approx(np.dot([1.0, 2.0, -1.0], (1 - cb) * sc_ + cb * co) * a * (1 - sig(0.3)),
+                                    abs=1e-13)
+
+
 def test_kat_texel_edge_is_inclusive():
     """tex_x == Wt-1 is sampled (hard cut is `x > W-1`, tile_common.h:177)."""
     t = np.zeros((8, 8), np.float32)
