@@ -45,6 +45,7 @@ SIGNATURES = {
     "dbmp_num_tiles": (_i, [_CP]),
     "dbmp_template_bboxes": (_i, [_vp, _i, _i, _i, _vp, _vp]),
     "dbmp_atlas_pack": (_i, [_vp, _i, _i, _i, _i, _vp, _vp]),
+    "dbmp_template_blur": (_i, [_vp, _i, _i, _i, _f, _vp, _vp]),
     "dbmp_atlas_bytes": (_sz, [_i, _i, _i, _i]),
     "dbmp_bin_workspace_bytes": (_sz, [_CP, _ll]),
     "dbmp_prim_info_bytes": (_sz, [_i]),

@@ -508,6 +508,60 @@ int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* 
   return launch_atlas_grid(tmpl, P, Ht, Wt, kind, out, st);
 }
 
+// Gaussian blur of the templates (pydiffbmp/util/utils.py:22-67,
+// gaussian_blur, as vector_renderer.py:80-96 applies it to the atlas): a K x K
+// kernel, K = 2 round(3 sigma) + 1, weights k[i] k[j] of the normalised 1-D
+// Gaussian exp(-0.5 ((i - K/2) / sigma)^2), zero padding, same output size.
+// One thread per output texel; the 1-D weights sit in shared memory.
+__global__ void template_blur_kernel(const float* __restrict__ in, int P, int Ht, int Wt, int K, float sigma,
+                                     float* __restrict__ out) {
+  extern __shared__ float s_k[];
+  if (threadIdx.x == 0) {
+    float sum = 0.f;
+    for (int i = 0; i < K; ++i) {
+      const float a = (float)(i - K / 2) / sigma;
+      s_k[i] = expf(-0.5f * (a * a));
+      sum += s_k[i];
+    }
+    for (int i = 0; i < K; ++i) s_k[i] /= sum;
+  }
+  __syncthreads();
+  const long long total = (long long)P * Ht * Wt;
+  const int h = K / 2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(t % Wt), y = (int)((t / Wt) % Ht);
+    const float* src = in + (t - (long long)y * Wt - x);
+    float acc = 0.f;
+    for (int i = 0; i < K; ++i) {
+      const int yy = y + i - h;
+      if (yy < 0 || yy >= Ht) continue;
+      for (int j = 0; j < K; ++j) {
+        const int xx = x + j - h;
+        if (xx < 0 || xx >= Wt) continue;
+        acc = fmaf(s_k[i] * s_k[j], src[(size_t)yy * Wt + xx], acc);
+      }
+    }
+    out[t] = acc;
+  }
+}
+
+int launch_template_blur(const float* in, int P, int Ht, int Wt, float sigma, float* out, cudaStream_t st) {
+  const long long total = (long long)P * Ht * Wt;
+  if (total == 0) return DBMP_OK;
+  if (!(sigma > 0.f)) {   // sigma <= 0 leaves the templates unchanged (utils.py:37-38)
+    if (in == out) return DBMP_OK;
+    cudaError_t e = cudaMemcpyAsync(out, in, sizeof(float) * (size_t)total, cudaMemcpyDeviceToDevice, st);
+    return e == cudaSuccess ? DBMP_OK : cuda_status(e, "cudaMemcpyAsync(templates)");
+  }
+  // K = 2 * round(3 sigma) + 1 with Python's round (ties to even), as rint does
+  const int K = (int)(2.0 * rint(3.0 * (double)sigma) + 1.0);
+  if (K > 4097) { set_error("dbmp_template_blur: sigma %g gives a kernel of %d texels", (double)sigma, K); return DBMP_ERR_INVALID; }
+  const int blocks = (int)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16);
+  template_blur_kernel<<<blocks, 256, sizeof(float) * K, st>>>(in, P, Ht, Wt, K, sigma, out);
+  DBMP_CHECK_LAUNCH("template_blur_kernel");
+  return DBMP_OK;
+}
+
 int launch_prepare(const Geom& g, const float* means2D, const float* radii, const float* rot, const float* opac,
                    const float* colors, const int* sel, PrimInfo* out, cudaStream_t st) {
   if (g.N == 0) return DBMP_OK;

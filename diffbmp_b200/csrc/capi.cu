@@ -25,6 +25,7 @@ int cuda_status(cudaError_t e, const char* what) {
 size_t bin_workspace_bytes(int N, int T, int tilesX, int tilesY, long long cap);
 size_t atlas_bytes(int P, int Ht, int Wt, int kind);
 int launch_template_bboxes(const float* tmpl, int P, int Ht, int Wt, float* out, cudaStream_t st);
+int launch_template_blur(const float* in, int P, int Ht, int Wt, float sigma, float* out, cudaStream_t st);
 int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* out, cudaStream_t st);
 int launch_prepare(const Geom& g, const float* means2D, const float* radii, const float* rot, const float* opac,
                    const float* colors, const int* sel, PrimInfo* out, cudaStream_t st);
@@ -134,6 +135,13 @@ int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* o
   REQUIRE(P >= 0 && Ht >= 2 && Wt >= 2, "dbmp_template_bboxes: bad atlas shape %dx%dx%d", P, Ht, Wt);
   REQUIRE(P == 0 || (templates && out_bbox), "dbmp_template_bboxes: null pointer");
   return launch_template_bboxes(templates, P, Ht, Wt, out_bbox, (cudaStream_t)stream);
+}
+
+int dbmp_template_blur(const float* templates, int P, int Ht, int Wt, float sigma, float* out, void* stream) {
+  REQUIRE(P >= 0 && Ht >= 1 && Wt >= 1, "dbmp_template_blur: bad atlas shape %dx%dx%d", P, Ht, Wt);
+  REQUIRE(P == 0 || (templates && out), "dbmp_template_blur: null pointer");
+  REQUIRE(templates != out || !(sigma > 0.f), "dbmp_template_blur: in-place blur is not supported");
+  return launch_template_blur(templates, P, Ht, Wt, sigma, out, (cudaStream_t)stream);
 }
 
 int dbmp_atlas_pack(const float* templates, int P, int Ht, int Wt, int kind, void* out, void* stream) {

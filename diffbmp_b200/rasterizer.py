@@ -54,17 +54,26 @@ def _f32(t: torch.Tensor) -> torch.Tensor:
 
 
 class Atlas:
-    """Template atlas on the device.  ``templates``: (P,Ht,Wt) or (Ht,Wt)."""
+    """Template atlas on the device.  ``templates``: (P,Ht,Wt) or (Ht,Wt).
+    ``sigma`` > 0 renders with Gaussian-blurred templates while the content
+    bboxes (binning) stay those of the unblurred ones, as the reference's
+    VectorRenderer does (vector_renderer.py:80-104)."""
 
-    def __init__(self, templates: torch.Tensor, kind: str | int = "f32"):
+    def __init__(self, templates: torch.Tensor, kind: str | int = "f32", sigma: float = 0.0):
         t = templates if templates.dim() == 3 else templates.unsqueeze(0)
         _need_cuda(t)
         self.templates = _f32(t)
+        self.sigma = float(sigma)
         self.P, self.Ht, self.Wt = (int(v) for v in self.templates.shape)
         self.kind = KIND_NAMES[kind] if isinstance(kind, str) else int(kind)
         st = _stream()
         self.bbox = torch.empty((self.P, 4), dtype=torch.float32, device=t.device)
         call("dbmp_template_bboxes", _ptr(self.templates), self.P, self.Ht, self.Wt, _ptr(self.bbox), st)
+        if self.sigma > 0.0:
+            blurred = torch.empty_like(self.templates)
+            call("dbmp_template_blur", _ptr(self.templates), self.P, self.Ht, self.Wt, ctypes.c_float(self.sigma),
+                 _ptr(blurred), st)
+            self.templates = blurred
         if self.kind == ATLAS_F32:
             self.data = self.templates
         else:
@@ -73,7 +82,9 @@ class Atlas:
             call("dbmp_atlas_pack", _ptr(self.templates), self.P, self.Ht, self.Wt, self.kind, _ptr(self.data), st)
 
     def with_kind(self, kind) -> "Atlas":
-        return Atlas(self.templates, kind)
+        a = Atlas(self.templates, kind)
+        a.bbox, a.sigma = self.bbox, self.sigma   # keep the unblurred content bboxes
+        return a
 
 
 @dataclass

@@ -76,6 +76,16 @@ int dbmp_num_tiles(const dbmp_canvas* cv);
 int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* out_bbox,
                          void* stream);
 
+/* Gaussian blur of a (P,Ht,Wt) f32 atlas into out (same shape, not in
+ * place): kernel size K = 2 round(3 sigma) + 1 (ties to even), weights the
+ * outer product of the normalised 1-D Gaussian, zero padding; sigma <= 0
+ * copies.  Replaces gaussian_blur (pydiffbmp/util/utils.py:22-67) as
+ * VectorRenderer applies it to the templates it renders with
+ * (pydiffbmp/core/renderer/vector_renderer.py:80-96); the content bboxes
+ * stay those of the unblurred templates there (vector_renderer.py:103-104). */
+int dbmp_template_blur(const float* templates, int P, int Ht, int Wt, float sigma, float* out,
+                       void* stream);
+
 /* Repacks a (P,Ht,Wt) f32 atlas into a storage kind of the precision form:
  * *_QUAD: element (p,y,x) holds the bilinear neighbours t[y][x], t[y][x+1],
  *   t[y+1][x], t[y+1][x+1]; out holds P*Ht*Wt*4 elements;

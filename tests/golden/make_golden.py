@@ -13,6 +13,9 @@ the code paths exercised below.  Fixtures produced:
                      (pydiffbmp/core/renderer/simple_tile_renderer.py:130-171)
 * bin_<case>.npz  -- _unified_primitive_assignment + _convert_masks_to_mapping
                      (vector_renderer.py:401-444, simple_tile_renderer.py:721-766)
+* blur.npz         -- gaussian_blur (pydiffbmp/util/utils.py:22-67) of a small
+                     atlas at several sigmas, as VectorRenderer applies it
+                     (vector_renderer.py:80-96)
 * torch_<case>.npz -- the PyTorch per-tile renderer (_process_tiles_parallel with
                      CUDA off, simple_tile_renderer.py:479-569, 1304-1550):
                      image, alpha and autograd gradients of
@@ -188,6 +191,23 @@ def main():
     atlas_ns = np.stack([wl.random_shape(rng, 40)[:24, :] for _ in range(3)])  # 24x40, non-square
     gen_torch_case(str_, "ragged", 80, 96, 16, atlas_ns, 48, 22, 3.0, 25.0, 0.8)
     torch.set_num_threads(1)
+    gen_blur(args.reference)
+
+
+def gen_blur(ref_root):
+    import torch
+    from pydiffbmp.util.utils import gaussian_blur
+    from diffbmp_b200 import workloads as wl
+    rng = np.random.default_rng(13)
+    S = np.stack([wl.random_shape(rng, 40) for _ in range(3)]).astype(np.float32)
+    S[1, 3:9, 30:36] = 1.0                      # a hard-edged block
+    sigmas = np.array([0.5, 1.5, 2.0, 0.0], np.float32)
+    out = []
+    for sg in sigmas:
+        b = gaussian_blur(torch.from_numpy(S).unsqueeze(0), float(sg)).squeeze(0)
+        out.append(b.numpy().astype(np.float32))
+    np.savez_compressed(os.path.join(HERE, "blur.npz"), S=S, sigmas=sigmas, blurred=np.stack(out))
+    print("blur:", [float(np.abs(o - S).max()) for o in out])
 
 
 if __name__ == "__main__":

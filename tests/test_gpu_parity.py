@@ -331,3 +331,29 @@ def test_colour_map_blend_rejects_bad_input_gpu():
     with pytest.raises(ValueError):
         rz.forward(d["means2D"], d["radii"], d["rotations"], d["opacities"], d["colors"], d["sel"], atlas,
                    None, None, torch.zeros(3, device="cuda"), 0.5)
+
+
+# ---------------------------------------------------------------------------
+# template blur (the reference's gaussian_blur of the atlas)
+def test_template_blur_matches_reference_gpu():
+    """dbmp_template_blur against the reference's gaussian_blur run on the
+    fixture atlas (tests/golden/blur.npz), within float32 summation-order
+    rounding; Atlas(sigma=) renders with the blurred texels but bins with the
+    unblurred content bboxes, as VectorRenderer does."""
+    import ctypes
+    from diffbmp_b200._lib import call
+    gd = golden("blur")
+    S = torch.from_numpy(gd["S"]).cuda()
+    P, Ht, Wt = S.shape
+    for sg, want in zip(gd["sigmas"], gd["blurred"]):
+        out = torch.empty_like(S)
+        call("dbmp_template_blur", R._ptr(S), P, Ht, Wt, ctypes.c_float(float(sg)), R._ptr(out), R._stream())
+        err = (out.cpu() - torch.from_numpy(want)).abs().max().item()
+        print("sigma", float(sg), "max err", err)
+        assert err <= 2e-6
+    a = R.Atlas(S, "f32", sigma=1.5)
+    a0 = R.Atlas(S, "f32")
+    assert torch.equal(a.bbox, a0.bbox)
+    assert (a.data.cpu() - torch.from_numpy(gd["blurred"][1])).abs().max().item() <= 2e-6
+    aq = a.with_kind("f16q")
+    assert torch.equal(aq.bbox, a0.bbox)
