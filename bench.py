@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c0", "c1", "c2"])
     ap.add_argument("--fast", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend under torchrun (gloo: the CPU-only reference arm)")
     ap.add_argument("--serving-jobs", type=int, default=48,
                     help="jobs of the serving stream measured beside the headline (0: skip)")
     ap.add_argument("--profile", default=None, choices=["f16", "f32", "bf16", "f32q", "f16q", "bf16q", "plain"],
@@ -62,7 +64,9 @@ def parse():
     return ap.parse_args()
 
 
-def dist_setup(args):
+def dist_setup(args, backend="nccl"):
+    """One process per GPU (torchrun env).  backend "gloo" runs the same
+    barrier / max-over-ranks plumbing without GPUs (used by the CPU tests)."""
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -70,10 +74,13 @@ def dist_setup(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    elif backend == "nccl" and torch.cuda.is_available():
         torch.cuda.set_device(0)
     return rank, world, local
 
@@ -89,7 +96,8 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -225,28 +233,41 @@ def counts(job, torch):
     return [int(v) for v in c.tolist()]
 
 
-def cpu_reference_sample(spec, rows, nthreads=0):
-    """Times the oracle port (reference algorithm) fwd+bwd on the first `rows`
-    tile rows; returns (seconds, rows_total)."""
-    from oracle import oracle as O
-    ts = 32
-    sc = O.Scene(spec.H, spec.W, ts, spec.means2D, spec.radii, spec.rotations, spec.opacities, spec.colors,
-                 spec.templates, spec.sel, spec.alpha_max)
-    tb = O.template_bboxes(spec.templates)
-    P, Ht, Wt = spec.templates.shape
-    offs, idx = O.bin_tiles(spec.H, spec.W, ts, spec.means2D, spec.radii, spec.rotations, spec.sel, tb, Ht, Wt)
-    tiles_x = (spec.W + ts - 1) // ts
-    rows_total = (spec.H + ts - 1) // ts
-    Hs = min(spec.H, rows * ts)
-    sub = O.Scene(Hs, spec.W, ts, sc.means2D, sc.radii, sc.rot, sc.opac, sc.colors, sc.templates, sc.sel,
-                  sc.alpha_max)
-    so = offs[: rows * tiles_x + 1]
-    si = idx[: so[-1]]
-    gc = np.ones((Hs, spec.W, 3), np.float32) * 1e-3
-    t0 = time.perf_counter()
-    O.forward(sub, so, si, nthreads=nthreads)
-    O.backward(sub, so, si, gc, None, nthreads=nthreads)
-    return time.perf_counter() - t0, rows_total
+class CpuReference:
+    """The reference algorithm on the host cores through the oracle port
+    (FP64, all host threads, no early termination).  Bins the scene once;
+    sample(px_rows) times forward + backward over the first px_rows pixel rows
+    and returns the time extrapolated to the whole canvas."""
+
+    def __init__(self, spec, ts=32):
+        from oracle import oracle as O
+        self.O, self.spec, self.ts = O, spec, ts
+        self.sc = O.Scene(spec.H, spec.W, ts, spec.means2D, spec.radii, spec.rotations, spec.opacities,
+                          spec.colors, spec.templates, spec.sel, spec.alpha_max)
+        tb = O.template_bboxes(spec.templates)
+        P, Ht, Wt = spec.templates.shape
+        self.offs, self.idx = O.bin_tiles(spec.H, spec.W, ts, spec.means2D, spec.radii, spec.rotations, spec.sel,
+                                          tb, Ht, Wt)
+        self.tiles_x = (spec.W + ts - 1) // ts
+
+    def sample(self, px_rows, nthreads=0):
+        O, sc, spec, ts = self.O, self.sc, self.spec, self.ts
+        Hs = max(1, min(spec.H, int(px_rows)))
+        sub = O.Scene(Hs, spec.W, ts, sc.means2D, sc.radii, sc.rot, sc.opac, sc.colors, sc.templates, sc.sel,
+                      sc.alpha_max)
+        so = self.offs[: ((Hs + ts - 1) // ts) * self.tiles_x + 1]
+        si = self.idx[: so[-1]]
+        gc = np.ones((Hs, spec.W, 3), np.float32) * 1e-3
+        t0 = time.perf_counter()
+        O.forward(sub, so, si, nthreads=nthreads)
+        O.backward(sub, so, si, gc, None, nthreads=nthreads)
+        return (time.perf_counter() - t0) * spec.H / Hs
+
+    def rows_for_budget(self, seconds_per_sample):
+        """Pixel rows per sample so that one sample takes about the given time."""
+        t1 = self.sample(1)                       # whole-canvas time estimated from one row
+        per_row = t1 / self.spec.H
+        return int(min(self.spec.H, max(1, seconds_per_sample / max(per_row, 1e-9))))
 
 
 def run_serving(n_jobs, seed, torch):
@@ -282,32 +303,40 @@ def run_serving(n_jobs, seed, torch):
 def run_reference(args):
     """--impl reference: the reference algorithm on the host cores (oracle port)."""
     import torch
-    rank, world, _ = dist_setup(args)
+    rank, world, _ = dist_setup(args, args.dist_backend)
     if rank != 0:
         barrier(world)
+        finish(world)
         return
     from diffbmp_b200 import workloads as wl
     spec = wl.make_scene(args.config, seed=0)
     cores = os.cpu_count() or 1
-    rows = 1
+    ref = CpuReference(spec)
+    # each step is a bounded sample (a band of pixel rows) so that the whole
+    # run stays within about two minutes whatever --steps / --warmup are
+    rows = ref.rows_for_budget(min(2.0, 120.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_reference_sample(spec, rows)
-    times = []
-    for _ in range(args.steps):
-        t, rows_total = cpu_reference_sample(spec, rows)
-        times.append(t * rows_total / rows)
+        ref.sample(rows)
+    times = [ref.sample(rows) for _ in range(args.steps)]
     per_iter = float(np.median(times))
     value = 1.0 / per_iter
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.config}: reference fwd+bwd on host cores, extrapolated from {rows} tile row(s) "
-                                   f"of 32 px per step", "canvas": [spec.H, spec.W], "N": spec.N},
+            "config": {"workload": f"{args.config}: reference fwd+bwd on host cores, extrapolated from {rows} "
+                                   f"pixel row(s) per step", "canvas": [spec.H, spec.W], "N": spec.N},
             "cpu_baseline": {"value": value, "unit": "iters/s", "cores": cores, "kind": "port",
-                             "sample": f"{rows} of {(spec.H + 31) // 32} tile rows per step, fwd+bwd, extrapolated"},
+                             "sample": f"{rows} of {spec.H} pixel rows per step, fwd+bwd, extrapolated"},
             "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     barrier(world)
+    finish(world)
+
+
+def finish(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def main():
@@ -352,11 +381,9 @@ def main():
     fused32 = build_job(spec, "f32", True, torch)
     t_fused32, _ = time_steps(fused32, args.steps, args.warmup, torch, world)
     t_fused32 = max_over_ranks(t_fused32, world)
-    del fused32
     pair = build_job(spec, "f16", True, torch)
     t_pair, _ = time_steps(pair, args.steps, args.warmup, torch, world)
     t_pair = max_over_ranks(t_pair, world)
-    del pair
 
     # --- e2e through the public API with host buffers ---------------------
     e2e_job = build_job(spec, HEADLINE_KIND, True, torch)
@@ -439,19 +466,22 @@ def main():
                              "(+ one memset and the two kernels of one CUB exclusive scan over the tile counts)",
         "clocks": clocks,
     }
-    if args.serving_jobs > 0:
+    if args.serving_jobs > 0 and world == 1:   # the serving stream is a single-GPU measurement
         line["serving"] = run_serving(args.serving_jobs, rank, torch)
     if rank == 0 and world == 1 and not args.fast:
-        t_cpu, rows_total = cpu_reference_sample(spec, 1)
-        line["cpu_baseline"] = {"value": 1.0 / (t_cpu * rows_total), "unit": "iters/s", "cores": os.cpu_count(),
+        ref = CpuReference(spec)
+        rows = ref.rows_for_budget(15.0)          # about 15 s of CPU work
+        t_cpu = ref.sample(rows)
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "iters/s", "cores": os.cpu_count(),
                                 "kind": "port",
-                                "sample": f"oracle fwd+bwd (reference algorithm, FP64, no termination) on 1 of "
-                                          f"{rows_total} tile rows, x{rows_total} extrapolated"}
+                                "sample": f"oracle fwd+bwd (reference algorithm, FP64, no termination) on {rows} of "
+                                          f"{spec.H} pixel rows, extrapolated to the canvas"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
-        job.graph = None; plain.graph = None; fused32.graph = None
+        for j in (job, plain, fused32, pair, e2e_job):
+            j.graph = None
         dist.barrier()
         dist.destroy_process_group()
 
