@@ -85,7 +85,7 @@ class Server:
     the precision form, "f32" plain); ``fused``: fused fwd/bwd kernel."""
 
     def __init__(self, atlas_templates: torch.Tensor, kind="f16", fused=True, max_slots=48,
-                 hbm_budget=150e9, n_streams=16, depth=2, graphs=True, lr=0.01, keep_params=False):
+                 hbm_budget=150e9, n_streams=16, depth=3, graphs=True, lr=0.01, keep_params=False):
         self.atlas = Atlas(atlas_templates, kind)
         self.cfg = FitConfig(lr=lr, fused=fused)
         self.max_slots = max_slots
@@ -114,7 +114,8 @@ class Server:
         used = 0
         t0 = time.perf_counter()
         clock = lambda: time.perf_counter() - t0
-        rr = 0
+        load = {id(st): 0 for st in self.streams}        # active jobs per stream
+        inflight = collections.deque()                   # events of issued iterations, in issue order
         while pending or active:
             now = clock()
             # admission: arrived jobs, while slots and the HBM budget allow
@@ -123,8 +124,10 @@ class Server:
                 if used + est > self.budget and active:
                     break
                 req = pending.popleft()
-                slot = self._admit(req, max(now, req.arrival) if realtime else now, self.streams[rr % len(self.streams)])
-                rr += 1
+                # the least-loaded stream: a new job does not queue behind several others
+                stream = min(self.streams, key=lambda st: load[id(st)])
+                load[id(stream)] += 1
+                slot = self._admit(req, max(now, req.arrival) if realtime else now, stream)
                 slot.nbytes = est
                 used += est
                 active.append(slot)
@@ -146,6 +149,7 @@ class Server:
                     results.append(JobResult(slot.req.job_id, arrival, slot.admitted, clock(), loss,
                                              replayed, params))
                     active.remove(slot)
+                    load[id(slot.stream)] -= 1
                     used -= slot.nbytes
                     progressed = True
                     continue
@@ -156,14 +160,17 @@ class Server:
                         ev = torch.cuda.Event()
                         ev.record(slot.stream)
                     slot.events.append(ev)
+                    inflight.append(ev)
                     slot.issued += 1
                     progressed = True
             if not progressed:
                 if active:
-                    # nothing to issue: wait for the oldest in-flight iteration
-                    oldest = min((s for s in active if s.events), key=lambda s: s.issued, default=None)
-                    if oldest is not None:
-                        oldest.events[0].synchronize()
+                    # nothing to issue: wait for the earliest-issued iteration still
+                    # running (the device retires work roughly in issue order)
+                    while inflight and inflight[0].query():
+                        inflight.popleft()
+                    if inflight:
+                        inflight.popleft().synchronize()
                     else:
                         time.sleep(0.0002)
                 elif pending and realtime:
