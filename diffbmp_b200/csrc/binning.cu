@@ -51,14 +51,20 @@ __global__ void template_bbox_kernel(const float* __restrict__ tmpl, int Ht, int
 }
 
 // ---------------------------------------------------------------------------
-// Atlas repacking into bilinear quads (precision form).
+// Atlas repacking into bilinear quads / pairs (precision form).  Each record
+// holds a texel and the difference to its right neighbour, the difference
+// taken against the stored (rounded) texel, so that stored texel + stored
+// difference is the neighbour up to one rounding of the difference.
 template <typename OutT>
 __device__ __forceinline__ OutT to_storage(float v);
 template <> __device__ __forceinline__ float to_storage<float>(float v) { return v; }
 template <> __device__ __forceinline__ __half to_storage<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 to_storage<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+__device__ __forceinline__ float from_storage(float v) { return v; }
+__device__ __forceinline__ float from_storage(__half v) { return __half2float(v); }
+__device__ __forceinline__ float from_storage(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-// Pair layout: (P, Ht+1, Wt) records of (t[y][x], t[y][x+1]); row Ht is zero.
+// Pair layout: (P, Ht+1, Wt) records of (t[y][x], t[y][x+1] - t[y][x]); row Ht is zero.
 template <typename OutT>
 __global__ void atlas_pair_kernel(const float* __restrict__ tmpl, int P, int Ht, int Wt, OutT* __restrict__ out) {
   const long long total = (long long)P * (Ht + 1) * Wt;
@@ -69,11 +75,14 @@ __global__ void atlas_pair_kernel(const float* __restrict__ tmpl, int P, int Ht,
     const float* t = tmpl + (size_t)p * Ht * Wt;
     const float v0 = (y < Ht) ? t[(size_t)y * Wt + x] : 0.f;
     const float v1 = (y < Ht && x + 1 < Wt) ? t[(size_t)y * Wt + x + 1] : 0.f;
-    out[2 * i] = to_storage<OutT>(v0);
-    out[2 * i + 1] = to_storage<OutT>(v1);
+    const OutT s0 = to_storage<OutT>(v0);
+    out[2 * i] = s0;
+    out[2 * i + 1] = to_storage<OutT>(v1 - from_storage(s0));
   }
 }
 
+// Quad layout: (P, Ht, Wt) records of (t[y][x], t[y][x+1] - t[y][x], t[y+1][x],
+// t[y+1][x+1] - t[y+1][x]); neighbours outside the template are 0.
 template <typename OutT>
 __global__ void atlas_pack_kernel(const float* __restrict__ tmpl, int P, int Ht, int Wt, OutT* __restrict__ out) {
   const long long total = (long long)P * Ht * Wt;
@@ -87,8 +96,9 @@ __global__ void atlas_pack_kernel(const float* __restrict__ tmpl, int P, int Ht,
     const float v10 = yr ? t[(size_t)(y + 1) * Wt + x] : 0.f;
     const float v11 = (xr && yr) ? t[(size_t)(y + 1) * Wt + x + 1] : 0.f;
     OutT* o = out + 4 * i;
-    o[0] = to_storage<OutT>(v00); o[1] = to_storage<OutT>(v01);
-    o[2] = to_storage<OutT>(v10); o[3] = to_storage<OutT>(v11);
+    const OutT s00 = to_storage<OutT>(v00), s10 = to_storage<OutT>(v10);
+    o[0] = s00; o[1] = to_storage<OutT>(v01 - from_storage(s00));
+    o[2] = s10; o[3] = to_storage<OutT>(v11 - from_storage(s10));
   }
 }
 

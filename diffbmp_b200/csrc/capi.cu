@@ -82,6 +82,7 @@ int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
     return DBMP_ERR_INVALID;
   }
   if (cv->atlas_kind < DBMP_ATLAS_F32 || cv->atlas_kind > DBMP_ATLAS_BF16_PAIR) { set_error("%s: atlas_kind %d unknown", who, cv->atlas_kind); return DBMP_ERR_INVALID; }
+  if (!(cv->alpha_max >= 0.f && cv->alpha_max < INFINITY)) { set_error("%s: alpha_max %g is not a finite value >= 0", who, (double)cv->alpha_max); return DBMP_ERR_INVALID; }
   if (!(cv->t_stop >= 1e-30f && cv->t_stop < 1.f)) { set_error("%s: t_stop %g outside [1e-30, 1)", who, (double)cv->t_stop); return DBMP_ERR_INVALID; }
   if ((long long)cv->height * cv->width > (1ll << 31) / 4) { set_error("%s: canvas too large", who); return DBMP_ERR_INVALID; }
   g->H = cv->height; g->W = cv->width; g->TS = cv->tile_size;
@@ -93,6 +94,13 @@ int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
   g->hy = 0.5f * (float)(cv->tmpl_h - 1);
   g->rxy = g->hx / g->hy;
   g->ryx = g->hy / g->hx;
+  g->k23 = make_float2(8388608.f, 8388608.f);
+  g->m1 = make_float2(-1.f, -1.f);
+  g->nhx = make_float2(-g->hx, -g->hx);
+  g->nhy = make_float2(-g->hy, -g->hy);
+  g->rxy2 = make_float2(g->rxy, g->rxy);
+  g->nryx2 = make_float2(-g->ryx, -g->ryx);
+  g->kbias = 0x4B000000u * (unsigned)(cv->tmpl_w + 1);
   g->wm1 = (float)(cv->tmpl_w - 1);
   g->hm1 = (float)(cv->tmpl_h - 1);
   g->kind = cv->atlas_kind;

@@ -123,6 +123,12 @@ template <> struct DefaultNP<32> { static constexpr int v = DBMP_NP32; };
 template <> struct DefaultNP<16> { static constexpr int v = 1; };
 
 struct Geom {
+  // operand pairs of the packed pixel-pair arithmetic (both halves equal)
+  float2 k23;          // 2^23
+  float2 m1;           // -1
+  float2 nhx, nhy;     // -hx, -hy
+  float2 rxy2, nryx2;  // hx/hy, -hy/hx
+  unsigned kbias;      // 0x4B000000 (Wt + 1): the 2^23 bias of two floored coordinates in a record index
   int H, W, TS, tilesX, tilesY, T;
   int N, P, Ht, Wt;
   int kind;            // AtlasKind of the atlas the kernels read
@@ -137,29 +143,37 @@ struct Geom {
   long long grid_off;  // byte offset of the clearance grid in a packed atlas
 };
 
-// Bilinear neighbours (v00, v01, v10, v11) of texel (x0, y0); neighbours
-// outside the template read 0 (tile_common.h:188-194).
-struct Quad { float v00, v01, v10, v11; };
+// Bilinear neighbours of texel (x0, y0) in difference form: v00, d01 =
+// v01 - v00, v10, d11 = v11 - v10; neighbours outside the template read 0
+// (tile_common.h:188-194).  The packed kinds store this form; the reference
+// layout takes the differences after the loads.
+struct Quad { float v00, d01, v10, d11; };
 
 template <int KIND> struct AtlasFetch;
 
 template <> struct AtlasFetch<ATLAS_F32> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+  // the four neighbours as loaded: (v00, v01, v10, v11)
+  static __device__ __forceinline__ float4 get_raw(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     const float* t = static_cast<const float*>(atlas) + off + y0 * Wt + x0;
     const bool xr = x0 + 1 < Wt, yr = y0 + 1 < Ht;
-    Quad q;
-    q.v00 = __ldg(t);
-    q.v01 = xr ? __ldg(t + 1) : 0.f;
-    q.v10 = yr ? __ldg(t + Wt) : 0.f;
-    q.v11 = (xr && yr) ? __ldg(t + Wt + 1) : 0.f;
-    return q;
+    return make_float4(__ldg(t), xr ? __ldg(t + 1) : 0.f, yr ? __ldg(t + Wt) : 0.f,
+                       (xr && yr) ? __ldg(t + Wt + 1) : 0.f);
+  }
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    const float4 v = get_raw(atlas, off, Ht, Wt, x0, y0);
+    return Quad{v.x, v.y - v.x, v.z, v.w - v.z};
   }
 };
 
 template <> struct AtlasFetch<ATLAS_F32_QUAD> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
-    const float4 v = __ldg(static_cast<const float4*>(atlas) + off + y0 * Wt + x0);
+  // record i (= off + y0 Wt + x0; int or unsigned)
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+    const float4 v = __ldg(static_cast<const float4*>(atlas) + i);
     return Quad{v.x, v.y, v.z, v.w};
+  }
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
@@ -169,34 +183,50 @@ __device__ __forceinline__ float2 b2f(unsigned u) {
 }
 
 template <> struct AtlasFetch<ATLAS_F16_QUAD> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
-    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + off + y0 * Wt + x0);
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + i);
     const float2 a = h2f(raw.x), b = h2f(raw.y);
     return Quad{a.x, a.y, b.x, b.y};
+  }
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
 template <> struct AtlasFetch<ATLAS_BF16_QUAD> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
-    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + off + y0 * Wt + x0);
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + i);
     const float2 a = b2f(raw.x), b = b2f(raw.y);
     return Quad{a.x, a.y, b.x, b.y};
+  }
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
 template <> struct AtlasFetch<ATLAS_F16_PAIR> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
-    const unsigned* p = static_cast<const unsigned*>(atlas) + off + y0 * Wt + x0;
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+    const unsigned* p = static_cast<const unsigned*>(atlas) + i;
     const float2 a = h2f(__ldg(p)), b = h2f(__ldg(p + Wt));   // row Ht is the zero pad
     return Quad{a.x, a.y, b.x, b.y};
+  }
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
 template <> struct AtlasFetch<ATLAS_BF16_PAIR> {
-  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
-    const unsigned* p = static_cast<const unsigned*>(atlas) + off + y0 * Wt + x0;
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+    const unsigned* p = static_cast<const unsigned*>(atlas) + i;
     const float2 a = b2f(__ldg(p)), b = b2f(__ldg(p + Wt));
     return Quad{a.x, a.y, b.x, b.y};
+  }
+  static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
+    return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
@@ -206,33 +236,6 @@ __device__ __forceinline__ int floor_small(float v, float* fl) {
   const float b = __fadd_rz(v, 8388608.f);
   *fl = b - 8388608.f;
   return __float_as_int(b) - 0x4B000000;
-}
-
-// Template mask at texel coordinate (tx, ty) of the template starting at
-// `off`: bilinear with a hard zero outside [0,Wt-1]x[0,Ht-1]
-// (tile_common.h:175-198), clamped to [0,1] (tile_forward.cu:271).  NaN
-// coordinates never reach here (kSolid primitives are handled by the caller).
-// With GRAD also returns d(mask)/d(tex) before the clamp (tile_common.h:201-239).
-template <int KIND, bool GRAD>
-__device__ __forceinline__ float sample_mask(const void* atlas, int off, const Geom& g, float tx, float ty,
-                                             float* gx, float* gy) {
-  if (!(tx >= 0.f && tx <= g.wm1 && ty >= 0.f && ty <= g.hm1)) {
-    if (GRAD) { *gx = 0.f; *gy = 0.f; }
-    return 0.f;
-  }
-  float fx, fy;
-  const int x0 = floor_small(tx, &fx), y0 = floor_small(ty, &fy);
-  const float wx = tx - fx, wy = ty - fy;
-  const Quad q = AtlasFetch<KIND>::get(atlas, off, g.Ht, g.Wt, x0, y0);
-  const float dt = q.v01 - q.v00, db = q.v11 - q.v10;
-  const float top = fmaf(wx, dt, q.v00);
-  const float bot = fmaf(wx, db, q.v10);
-  const float m = fmaf(wy, bot - top, top);
-  if (GRAD) {
-    *gx = fmaf(wy, db - dt, dt);
-    *gy = bot - top;
-  }
-  return fmaxf(0.f, fminf(1.f, m));
 }
 
 __device__ __forceinline__ float sigmoid_precise(float x) {

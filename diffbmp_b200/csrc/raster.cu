@@ -1,7 +1,7 @@
 // Forward / backward / fused tile compositing kernels.
 //
 // A tile of TS x TS pixels is walked by NW warps (one or more CTAs); each thread owns NP pixels
-// (NP = 4, 2 or 1) of a compact warp footprint (16x8, 16x4 or 8x4 pixels) so
+// (NP = 4, 2 or 1) of a compact warp footprint (16x8, 8x8 or 8x4 pixels) so
 // that a primitive's square cull is mostly warp-uniform and the warp's texel
 // fetches stay close together in the atlas.
 //
@@ -126,10 +126,13 @@ __device__ __forceinline__ void entry_sample(const Geom& g, const void* __restri
   }
 }
 
-// Bilinear mask (clamped) and, with GRAD, its texel-space gradient.
+// Bilinear mask and, with GRAD, its texel-space gradient.  The reference
+// clamps the mask to [0,1] (tile_forward.cu:271, NaN -> 1); only the upper
+// clamp is applied here, since every caller discards masks failing the
+// fragment test mask > 1e-6, which the lower clamp cannot change.
 template <bool GRAD>
 __device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
-  const float dt = s.q.v01 - s.q.v00, db = s.q.v11 - s.q.v10;
+  const float dt = s.q.d01, db = s.q.d11;
   const float top = fmaf(s.wx, dt, s.q.v00);
   const float bot = fmaf(s.wx, db, s.q.v10);
   const float m = fmaf(s.wy, bot - top, top);
@@ -137,7 +140,85 @@ __device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
     *gx = fmaf(s.wy, db - dt, dt);
     *gy = bot - top;
   }
-  return fmaxf(0.f, fminf(1.f, m));
+  return fminf(1.f, m);
+}
+
+// ---------------------------------------------------------------------------
+// Pixel pairs.  With 2 pixels per thread the per-entry arithmetic of both
+// pixels runs as one float2 (x: pixel 0, y: pixel 1) through the packed FP32x2
+// instructions of sm_100, one instruction for both pixels.  Each packed
+// operation rounds exactly like its scalar counterpart; constant operands come
+// as pairs from the kernel parameters (Geom) or the staged record.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// b - a, as the exact FMA a * -1 + b
+__device__ __forceinline__ float2 sub2(const Geom& g, float2 b, float2 a) { return __ffma2_rn(a, g.m1, b); }
+
+// Texel coordinates, sampling weights and neighbours of a thread's two pixels.
+struct PairSample {
+  float2 tx, ty;             // texel coordinates (not redirected)
+  float2 wx, wy;             // bilinear weights of the fetched texel
+  float2 v00, d01, v10, d11;  // neighbours in difference form (Quad)
+  bool ok0, ok1;             // pixel can yield a fragment (as Sample::ok)
+};
+
+template <class L, int KIND, bool FAST>
+__device__ __forceinline__ void pair_sample(const Geom& g, const void* __restrict__ atlas, int toff,
+                                            const float4& g0, const float4& g1, bool inside, const float (&pxf)[2],
+                                            const float (&pyf)[2], const bool (&live)[2], PairSample& s) {
+  Sample c[2];
+  entry_coords<2, L, FAST>(g, g0, g1, inside, pxf, pyf, live, c);
+  s.ok0 = c[0].ok;
+  s.ok1 = c[1].ok;
+  s.tx = make_float2(c[0].tx, c[1].tx);
+  s.ty = make_float2(c[0].ty, c[1].ty);
+  // pixels without a fragment sample texel 0 of the template (in bounds)
+  const float2 tx = FAST ? s.tx : make_float2(c[0].ok ? c[0].tx : 0.f, c[1].ok ? c[1].tx : 0.f);
+  const float2 ty = FAST ? s.ty : make_float2(c[0].ok ? c[0].ty : 0.f, c[1].ok ? c[1].ty : 0.f);
+  // floor as in floor_small: adding 2^23 rounding toward zero
+  const float2 bx = __fadd2_rz(tx, g.k23), by = __fadd2_rz(ty, g.k23);
+  const float2 fx = fma2(g.m1, g.k23, bx), fy = fma2(g.m1, g.k23, by);
+  s.wx = sub2(g, tx, fx);
+  s.wy = sub2(g, ty, fy);
+  if constexpr (KIND == ATLAS_F32) {
+    // reference layout: both pixels' differences as packed subtractions
+    const int x0 = __float_as_int(bx.x) - 0x4B000000, y0 = __float_as_int(by.x) - 0x4B000000;
+    const int x1 = __float_as_int(bx.y) - 0x4B000000, y1 = __float_as_int(by.y) - 0x4B000000;
+    const float4 r0 = AtlasFetch<KIND>::get_raw(atlas, toff, g.Ht, g.Wt, x0, y0);
+    const float4 r1 = AtlasFetch<KIND>::get_raw(atlas, toff, g.Ht, g.Wt, x1, y1);
+    s.v00 = make_float2(r0.x, r1.x);
+    s.v10 = make_float2(r0.z, r1.z);
+    s.d01 = sub2(g, make_float2(r0.y, r1.y), s.v00);
+    s.d11 = sub2(g, make_float2(r0.w, r1.w), s.v10);
+  } else {
+    // record index toff + y0 Wt + x0 straight from the biased bit patterns
+    // (2^23 + x0, 2^23 + y0): the bias is one constant per entry, and the
+    // unsigned arithmetic wraps back to the in-range index
+    const unsigned c = (unsigned)toff - g.kbias;
+    const Quad q0 = AtlasFetch<KIND>::at(atlas, __float_as_uint(by.x) * (unsigned)g.Wt + __float_as_uint(bx.x) + c, g.Wt);
+    const Quad q1 = AtlasFetch<KIND>::at(atlas, __float_as_uint(by.y) * (unsigned)g.Wt + __float_as_uint(bx.y) + c, g.Wt);
+    s.v00 = make_float2(q0.v00, q1.v00);
+    s.d01 = make_float2(q0.d01, q1.d01);
+    s.v10 = make_float2(q0.v10, q1.v10);
+    s.d11 = make_float2(q0.d11, q1.d11);
+  }
+}
+
+// Bilinear mask of both pixels (upper-clamped as in blend()) and, with GRAD, its texel-space
+// gradient: the operations of blend() on pairs.
+template <bool GRAD>
+__device__ __forceinline__ float2 pair_blend(const Geom& g, const PairSample& s, float2* gx, float2* gy) {
+  const float2 dt = s.d01, db = s.d11;
+  const float2 top = fma2(s.wx, dt, s.v00);
+  const float2 bot = fma2(s.wx, db, s.v10);
+  const float2 d = sub2(g, bot, top);
+  const float2 m = fma2(s.wy, d, top);
+  if (GRAD) {
+    *gx = fma2(s.wy, sub2(g, db, dt), dt);
+    *gy = d;
+  }
+  return make_float2(fminf(1.f, m.x), fminf(1.f, m.y));
 }
 
 // Colour-map sample (tile_forward.cu:17-89): the texel coordinate is clamped
@@ -175,12 +256,34 @@ struct ChunkMasks {
 
 // CB: fragment colours blend a per-primitive colour map (cmap, (N,Ht,Wt,3))
 // with weight cblend, (1 - cblend) sigmoid(c) + cblend c_o (tile_forward.cu:316-330).
+#ifndef DBMP_PACKED_PAIRS
+#define DBMP_PACKED_PAIRS 1
+#endif
+
+
 template <int TS, int NP, int KIND, bool CB = false>
 struct TileWalker {
   using L = Layout<TS, NP>;
   static constexpr int NT = L::NT;
   static constexpr int NW = L::NW;
   static constexpr bool kGrid = KIND != ATLAS_F32;   // packed atlases carry a clearance grid
+  // Pixel-pair walk (2 pixels per thread, fixed colours).  Its staged record
+  // holds the opacity and colours as duplicated pairs:
+  //   [0] (mx, my, hw, hh)  [1] A  [2] (op, op, r, r)  [3] (g, g, b, b)  [4] (toff, goff, gext, -)
+  // otherwise the PrimInfo record as is: [0] [1] A [2] (op, r, g, b) [3] (toff, goff, gext, -).
+  static constexpr bool kPair = DBMP_PACKED_PAIRS && NP == 2 && !CB;
+  static constexpr int kRec = kPair ? 5 : 4;
+  using Rec = float4[kRec];
+
+  // (op, r, g, b) and the atlas offset of a staged record.
+  static __device__ __forceinline__ float4 rec_g2(const Rec& r) {
+    if (kPair) {
+      const float4 a = r[2], b = r[3];
+      return make_float4(a.x, a.z, b.x, b.z);
+    }
+    return r[2];
+  }
+  static __device__ __forceinline__ int rec_toff(const Rec& r) { return __float_as_int(r[kRec - 1].x); }
 
   int warp, lw, lane, start, end;   // warp: index within the tile, lw: within the CTA
   const float* cmap = nullptr;
@@ -238,7 +341,7 @@ struct TileWalker {
   template <bool KEEP_CLEAR>
   __device__ __forceinline__ ChunkMasks stage(const Geom& g, const PrimInfo* __restrict__ prims,
                                               const int* __restrict__ idx, const unsigned char* __restrict__ grid,
-                                              int base, int stop, float4 (*w)[4], int* my_id) {
+                                              int base, int stop, Rec* w, int* my_id) {
     bool keep = false, inside = false, fast = false, clear = false, miss = false;
     int id = -1;
     __syncwarp();   // every lane is done with the previous chunk's records
@@ -269,10 +372,16 @@ struct TileWalker {
                 const float ey = fmaf(fabsf(g1.z), g.fhx, fmaf(fabsf(g1.w), g.fhy, 0.05f));
                 fast = cx - ex >= 0.f && cx + ex <= g.wm1 && cy - ey >= 0.f && cy + ey <= g.hm1;
               }
+              const float4 g2 = __ldg(r + 2);
               w[lane][0] = g0;
               w[lane][1] = g1;
-              w[lane][2] = __ldg(r + 2);
-              w[lane][3] = q;
+              if (kPair) {
+                w[lane][2] = make_float4(g2.x, g2.x, g2.y, g2.y);
+                w[lane][3] = make_float4(g2.z, g2.z, g2.w, g2.w);
+              } else {
+                w[lane][2] = g2;
+              }
+              w[lane][kRec - 1] = q;
             }
           }
         }
@@ -291,6 +400,193 @@ struct TileWalker {
     return m;
   }
 
+  // Adds the warp's 8 per-primitive sums (acc, one set per lane) to dst[0..7]:
+  // a recursive-halving reduction, 8 sums over 32 lanes in 9 shuffles, after
+  // which lane l < 8 holds sum kidx and adds it in FP64.
+  __device__ __forceinline__ void warp_add(float (&acc)[8], int kidx, double* __restrict__ dst) const {
+    const bool b0 = lane & 1, b1 = lane & 2, b2 = lane & 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float send = b0 ? acc[k] : acc[k + 4];
+      const float keep = b0 ? acc[k + 4] : acc[k];
+      acc[k] = keep + __shfl_xor_sync(kFull, send, 1);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const float send = b1 ? acc[k] : acc[k + 2];
+      const float keep = b1 ? acc[k + 2] : acc[k];
+      acc[k] = keep + __shfl_xor_sync(kFull, send, 2);
+    }
+    {
+      const float send = b2 ? acc[0] : acc[1];
+      const float keep = b2 ? acc[1] : acc[0];
+      acc[0] = keep + __shfl_xor_sync(kFull, send, 4);
+    }
+    acc[0] += __shfl_xor_sync(kFull, acc[0], 8);
+    acc[0] += __shfl_xor_sync(kFull, acc[0], 16);
+    if (lane < 8 && acc[0] != 0.f) atomicAdd(dst + kidx, (double)acc[0]);
+  }
+
+  // Forward walk of the pixel-pair form: the walk of forward() with both
+  // pixels' sampling, blending and compositing as packed pairs.
+  __device__ __forceinline__ void forward_pair(const Geom& g, const PrimInfo* __restrict__ prims,
+                                               const void* __restrict__ atlas, const int* __restrict__ idx, Rec* w,
+                                               float (&C)[2][3], float (&T)[2], float (&Tl)[2], int (&lp)[2]) {
+    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
+    bool live[2] = {valid[0], valid[1]};
+    float2 cr = make_float2(0.f, 0.f), cg = cr, cb = cr, t = make_float2(1.f, 1.f), tl = t;
+    int lp0 = -1, lp1 = -1;
+    bool warp_done = __all_sync(kFull, !live[0] && !live[1]);
+    for (int base = start; base < end && !warp_done; base += kChunk) {
+      int my_id;
+      const ChunkMasks cm = stage<false>(g, prims, idx, grid, base, end, w, &my_id);
+      unsigned todo = cm.todo;
+      while (todo) {
+        const int e = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const float4 g0 = w[e][0];
+        const float4 g1 = w[e][1];
+        const float4 c0 = w[e][2];
+        const float4 c1 = w[e][3];
+        const int toff = rec_toff(w[e]);
+        const int pos = base - start + e;
+        float2 m;
+        bool ok0, ok1;
+        if (toff != kSolid) {
+          PairSample s;
+          const bool inside = (cm.inside >> e) & 1u;
+          if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+          else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+          m = pair_blend<false>(g, s, nullptr, nullptr);
+          ok0 = s.ok0;
+          ok1 = s.ok1;
+        } else {
+          // NaN geometry: every live pixel that passes the cull gets mask 1
+          ok0 = live[0] && !(fabsf(pxf[0] - g0.x) > g0.z || fabsf(pyf[0] - g0.y) > g0.w);
+          ok1 = live[1] && !(fabsf(pxf[1] - g0.x) > g0.z || fabsf(pyf[1] - g0.y) > g0.w);
+          m = make_float2(1.f, 1.f);
+        }
+        const bool f0 = ok0 && m.x > 1e-6f, f1 = ok1 && m.y > 1e-6f;
+        float2 a = mul2(make_float2(c0.x, c0.y), m);
+        a.x = f0 ? a.x : 0.f;
+        a.y = f1 ? a.y : 0.f;
+        const float2 wt = mul2(t, a);
+        cr = fma2(wt, make_float2(c0.z, c0.w), cr);
+        cg = fma2(wt, make_float2(c1.x, c1.y), cg);
+        cb = fma2(wt, make_float2(c1.z, c1.w), cb);
+        tl.x = f0 ? t.x : tl.x;
+        tl.y = f1 ? t.y : tl.y;
+        lp0 = f0 ? pos : lp0;
+        lp1 = f1 ? pos : lp1;
+        // T (1 - a) as in forward(), saturated per pixel (no packed form)
+        t.x = __saturatef(fmaf(-t.x, a.x, t.x));
+        t.y = __saturatef(fmaf(-t.y, a.y, t.y));
+        live[0] = live[0] && !(t.x < g.t_stop);
+        live[1] = live[1] && !(t.y < g.t_stop);
+        if (__all_sync(kFull, !live[0] && !live[1])) { warp_done = true; break; }
+      }
+    }
+    C[0][0] = cr.x; C[0][1] = cg.x; C[0][2] = cb.x;
+    C[1][0] = cr.y; C[1][1] = cg.y; C[1][2] = cb.y;
+    T[0] = t.x; T[1] = t.y;
+    Tl[0] = tl.x; Tl[1] = tl.y;
+    lp[0] = lp0; lp[1] = lp1;
+  }
+
+  // Reverse walk of the pixel-pair form (the walk of backward() with both
+  // pixels' arithmetic as packed pairs; each per-primitive sum adds the two
+  // pixels' terms before the warp reduction).
+  __device__ __forceinline__ void backward_pair(const Geom& g, const PrimInfo* __restrict__ prims,
+                                                const void* __restrict__ atlas, const int* __restrict__ idx, Rec* w,
+                                                const float (&gC)[2][3], const float (&gA)[2], float (&Ts)[2],
+                                                const int (&lp)[2], double* __restrict__ gacc) {
+    const int warp_max = __reduce_max_sync(kFull, max(lp[0], lp[1]));
+    if (warp_max < 0) return;
+    const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
+    const int kidx = 4 * (lane & 1) + 2 * ((lane >> 1) & 1) + ((lane >> 2) & 1);
+    const float2 gcr = make_float2(gC[0][0], gC[1][0]), gcg = make_float2(gC[0][1], gC[1][1]),
+                 gcb = make_float2(gC[0][2], gC[1][2]), ga = make_float2(gA[0], gA[1]);
+    float2 h = make_float2(0.f, 0.f), bt = make_float2(1.f, 1.f), ts = make_float2(Ts[0], Ts[1]);
+    for (int cb = (warp_max / kChunk) * kChunk; cb >= 0; cb -= kChunk) {
+      int my_id;
+      const ChunkMasks cm = stage<false>(g, prims, idx, grid, start + cb, start + warp_max + 1, w, &my_id);
+      unsigned todo = cm.todo;
+      while (todo) {
+        const int e = 31 - __clz(todo);
+        todo &= ~(1u << e);
+        const int pos = cb + e;
+        const int id = __shfl_sync(kFull, my_id, e);
+        const float4 g0 = w[e][0];
+        const float4 g1 = w[e][1];
+        const float4 c0 = w[e][2];
+        const float4 c1 = w[e][3];
+        const int toff = rec_toff(w[e]);
+        const bool live[2] = {pos <= lp[0], pos <= lp[1]};
+        float2 m, gx, gy, tx, ty;
+        bool ok0, ok1;
+        if (toff != kSolid) {
+          PairSample s;
+          const bool inside = (cm.inside >> e) & 1u;
+          if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+          else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+          m = pair_blend<true>(g, s, &gx, &gy);
+          tx = s.tx;
+          ty = s.ty;
+          ok0 = s.ok0;
+          ok1 = s.ok1;
+        } else {
+          const float dx0 = pxf[0] - g0.x, dy0 = pyf[0] - g0.y, dx1 = pxf[1] - g0.x, dy1 = pyf[1] - g0.y;
+          ok0 = live[0] && !(fabsf(dx0) > g0.z || fabsf(dy0) > g0.w);
+          ok1 = live[1] && !(fabsf(dx1) > g0.z || fabsf(dy1) > g0.w);
+          tx = make_float2(fmaf(g1.x, dx0, fmaf(g1.y, dy0, g.hx)), fmaf(g1.x, dx1, fmaf(g1.y, dy1, g.hx)));
+          ty = make_float2(fmaf(g1.z, dx0, fmaf(g1.w, dy0, g.hy)), fmaf(g1.z, dx1, fmaf(g1.w, dy1, g.hy)));
+          m = make_float2(1.f, 1.f);
+          gx = gy = make_float2(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000));
+        }
+        const bool f0 = ok0 && m.x > 1e-6f, f1 = ok1 && m.y > 1e-6f;
+        float2 a = mul2(make_float2(c0.x, c0.y), m);
+        a.x = f0 ? a.x : 0.f;
+        a.y = f1 ? a.y : 0.f;
+        const float2 om = make_float2(__saturatef(1.f - a.x), __saturatef(1.f - a.y));
+        // T entering this fragment (see backward())
+        const float2 tk = make_float2((pos == lp[0]) ? ts.x : __fdividef(ts.x, om.x),
+                                      (pos == lp[1]) ? ts.y : __fdividef(ts.y, om.y));
+        ts = tk;
+        const float2 col_r = make_float2(c0.z, c0.w), col_g = make_float2(c1.x, c1.y),
+                     col_b = make_float2(c1.z, c1.w);
+        const float2 gcc = fma2(gcr, col_r, fma2(gcg, col_g, mul2(gcb, col_b)));
+        const float2 dlda = mul2(tk, fma2(ga, bt, sub2(g, gcc, h)));
+        const float2 u = mul2(dlda, make_float2(f0 ? gx.x : 0.f, f1 ? gx.y : 0.f));
+        const float2 v = mul2(dlda, make_float2(f0 ? gy.x : 0.f, f1 ? gy.y : 0.f));
+        const float2 ex = add2(tx, g.nhx), ey = add2(ty, g.nhy);
+        const float2 wt = mul2(a, tk);
+        float acc[8];
+        acc[0] = u.x + u.y;
+        acc[1] = v.x + v.y;
+        {
+          const float2 r = fma2(u, ex, mul2(v, ey));
+          acc[2] = r.x + r.y;
+        }
+        {
+          const float2 r = fma2(mul2(u, g.rxy2), ey, mul2(mul2(v, g.nryx2), ex));
+          acc[3] = r.x + r.y;
+        }
+        {
+          const float2 r4 = mul2(gcr, wt), r5 = mul2(gcg, wt), r6 = mul2(gcb, wt), r7 = mul2(dlda, a);
+          acc[4] = r4.x + r4.y;
+          acc[5] = r5.x + r5.y;
+          acc[6] = r6.x + r6.y;
+          acc[7] = r7.x + r7.y;
+        }
+        h = fma2(om, h, mul2(a, gcc));
+        bt = mul2(bt, om);
+        if (__any_sync(kFull, f0 || f1)) warp_add(acc, kidx, gacc + (size_t)id * 8);
+      }
+    }
+    Ts[0] = ts.x;
+    Ts[1] = ts.y;
+  }
+
   // Forward walk.  STATS: counts (pixel, primitive) pairs that pass the cull
   // and fragments composited, both before termination, plus walk statistics;
   // it evaluates the clearance-grid test without skipping and counts the
@@ -299,9 +595,13 @@ struct TileWalker {
   template <bool STATS = false>
   __device__ __forceinline__ void forward(const Geom& g, const PrimInfo* __restrict__ prims,
                                           const void* __restrict__ atlas, const int* __restrict__ idx,
-                                          float4 (*w)[4],
+                                          Rec* w,
                                           float (&C)[NP][3], float (&T)[NP], float (&Tl)[NP], int (&lp)[NP],
                                           unsigned long long* cnt = nullptr) {
+    if constexpr (kPair && !STATS) {
+      forward_pair(g, prims, atlas, idx, w, C, T, Tl, lp);
+      return;
+    }
     unsigned long long n_cand = 0, n_frag = 0, n_went = 0, n_slots = 0, n_miss = 0, n_empty = 0, n_clear = 0,
                        n_bad = 0;
     unsigned n_depth[NP];
@@ -327,8 +627,8 @@ struct TileWalker {
         todo &= todo - 1;
         const float4 g0 = w[e][0];
         const float4 g1 = w[e][1];
-        const float4 g2 = w[e][2];
-        const int toff = __float_as_int(w[e][3].x);
+        const float4 g2 = rec_g2(w[e]);
+        const int toff = rec_toff(w[e]);
         const int pos = base - start + e;
         const bool clear = (cm.clear >> e) & 1u;
         if (STATS) {
@@ -386,7 +686,9 @@ struct TileWalker {
           }
           Tl[p] = frag ? T[p] : Tl[p];
           lp[p] = frag ? pos : lp[p];
-          T[p] = fmaxf(fmaf(-T[p], a, T[p]), 0.f);   // T (1 - a), 0 when a > 1 (alpha_max > 1)
+          // T (1 - a); 0 when a > 1 (alpha_max > 1).  a >= 0 (alpha_max >= 0), so
+          // T stays <= 1 and saturating equals max(., 0), NaN included.
+          T[p] = __saturatef(fmaf(-T[p], a, T[p]));
           live[p] = live[p] && !(T[p] < g.t_stop);
           local_done = local_done && !live[p];
         }
@@ -418,8 +720,12 @@ struct TileWalker {
   // (layout documented at finalize_kernel).
   __device__ __forceinline__ void backward(const Geom& g, const PrimInfo* __restrict__ prims,
                                            const void* __restrict__ atlas, const int* __restrict__ idx,
-                                           float4 (*w)[4], const float (&gC)[NP][3], const float (&gA)[NP],
+                                           Rec* w, const float (&gC)[NP][3], const float (&gA)[NP],
                                            float (&Ts)[NP], const int (&lp)[NP], double* __restrict__ gacc) {
+    if constexpr (kPair) {
+      backward_pair(g, prims, atlas, idx, w, gC, gA, Ts, lp, gacc);
+      return;
+    }
     int my_max = -1;
 #pragma unroll
     for (int p = 0; p < NP; ++p) my_max = max(my_max, lp[p]);
@@ -449,8 +755,8 @@ struct TileWalker {
         const int id = __shfl_sync(kFull, my_id, e);
         const float4 g0 = w[e][0];
         const float4 g1 = w[e][1];
-        const float4 g2 = w[e][2];
-        const int toff = __float_as_int(w[e][3].x);
+        const float4 g2 = rec_g2(w[e]);
+        const int toff = rec_toff(w[e]);
         float acc[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) acc[k] = 0.f;
@@ -480,7 +786,7 @@ struct TileWalker {
         for (int p = 0; p < NP; ++p) {
           const bool frag = s[p].ok && m[p] > 1e-6f;
           const float a = frag ? g2.x * m[p] : 0.f;
-          const float om = fmaxf(1.f - a, 0.f);
+          const float om = __saturatef(1.f - a);   // max(1 - a, 0) for a >= 0
           // T entering this fragment: stored for the last contributor, else
           // undo the forward product (om >= t_stop > 0 for every earlier
           // fragment, so the fast division is well conditioned; om = 1 and
@@ -508,31 +814,7 @@ struct TileWalker {
           B[p] *= om;
           any = any || frag;
         }
-        if (__any_sync(kFull, any)) {
-          // recursive-halving reduction: 8 sums over 32 lanes in 9 shuffles;
-          // lane l (l < 8) ends with sum index kidx
-          const bool b0 = lane & 1, b1 = lane & 2, b2 = lane & 4;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const float send = b0 ? acc[k] : acc[k + 4];
-            const float keep = b0 ? acc[k + 4] : acc[k];
-            acc[k] = keep + __shfl_xor_sync(kFull, send, 1);
-          }
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const float send = b1 ? acc[k] : acc[k + 2];
-            const float keep = b1 ? acc[k + 2] : acc[k];
-            acc[k] = keep + __shfl_xor_sync(kFull, send, 2);
-          }
-          {
-            const float send = b2 ? acc[0] : acc[1];
-            const float keep = b2 ? acc[1] : acc[0];
-            acc[0] = keep + __shfl_xor_sync(kFull, send, 4);
-          }
-          acc[0] += __shfl_xor_sync(kFull, acc[0], 8);
-          acc[0] += __shfl_xor_sync(kFull, acc[0], 16);
-          if (lane < 8 && acc[0] != 0.f) atomicAdd(gacc + (size_t)id * 8 + kidx, (double)acc[0]);
-        }
+        if (__any_sync(kFull, any)) warp_add(acc, kidx, gacc + (size_t)id * 8);
       }
     }
   }
@@ -566,7 +848,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) forward_
     float* __restrict__ T_last, int* __restrict__ last_pos, const float* __restrict__ cmap, float cblend) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND, CB>;
-  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
+  __shared__ typename TW::Rec s_pi[kCtaWarps<TS>()][kChunk];
   TW tw;
   tw.cmap = cmap;
   tw.cblend = cblend;
@@ -598,7 +880,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>()) count_kernel(Geom g, const P
                                                                  unsigned long long* __restrict__ cnt) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
+  __shared__ typename TW::Rec s_pi[kCtaWarps<TS>()][kChunk];
   TW tw;
   const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
   tw.init(g, tile, part, kCtaWarps<TS>(), offs);
@@ -616,7 +898,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward
     const float* __restrict__ cmap, float cblend) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND, CB>;
-  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
+  __shared__ typename TW::Rec s_pi[kCtaWarps<TS>()][kChunk];
   TW tw;
   tw.cmap = cmap;
   tw.cblend = cblend;
@@ -698,7 +980,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_ke
   if (skip_flag != nullptr && *skip_flag != 0) return;   // binning overflowed: leave all state untouched
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND>;
-  __shared__ float4 s_pi[kCtaWarps<TS>()][kChunk][4];
+  __shared__ typename TW::Rec s_pi[kCtaWarps<TS>()][kChunk];
   __shared__ float s_loss[kCtaWarps<TS>()];
   __shared__ unsigned s_arrived;
   if (threadIdx.x == 0) s_arrived = 0u;

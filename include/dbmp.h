@@ -59,7 +59,7 @@ typedef struct {
   int32_t tmpl_h, tmpl_w;     /* Ht, Wt */
   int32_t atlas_kind;         /* DBMP_ATLAS_* */
   int32_t bin_mode;           /* DBMP_BIN_* */
-  float alpha_max;            /* alpha_upper_bound */
+  float alpha_max;            /* alpha_upper_bound (finite, >= 0) */
   float t_stop;               /* early-termination transmittance, in [1e-30, 1) */
   int32_t reserved;
 } dbmp_canvas;
@@ -86,12 +86,16 @@ int dbmp_template_bboxes(const float* templates, int P, int Ht, int Wt, float* o
 int dbmp_template_blur(const float* templates, int P, int Ht, int Wt, float sigma, float* out,
                        void* stream);
 
-/* Repacks a (P,Ht,Wt) f32 atlas into a storage kind of the precision form:
- * *_QUAD: element (p,y,x) holds the bilinear neighbours t[y][x], t[y][x+1],
- *   t[y+1][x], t[y+1][x+1]; out holds P*Ht*Wt*4 elements;
- * *_PAIR: element (p,y,x) holds t[y][x], t[y][x+1] for y < Ht plus one zero
- *   row y = Ht; out holds P*(Ht+1)*Wt*2 elements.
- * Neighbours outside the template are 0.  The texel records are followed,
+/* Repacks a (P,Ht,Wt) f32 atlas into a storage kind of the precision form,
+ * with each texel's right neighbour stored as a difference (the bilinear
+ * blend then needs no subtraction):
+ * *_QUAD: element (p,y,x) holds t[y][x], t[y][x+1] - t[y][x], t[y+1][x],
+ *   t[y+1][x+1] - t[y+1][x]; out holds P*Ht*Wt*4 elements;
+ * *_PAIR: element (p,y,x) holds t[y][x], t[y][x+1] - t[y][x] for y < Ht plus
+ *   one zero row y = Ht; out holds P*(Ht+1)*Wt*2 elements.
+ * Neighbours outside the template are 0; each difference is taken against
+ * the stored (rounded) texel, then rounded to the storage type.  The texel
+ * records are followed,
  * at the next 256-byte boundary, by a clearance grid: per template, cells of
  * 2^s x 2^t texels (s, t the smallest shifts giving at most 128 cells per
  * axis), one byte each, the L-infinity distance in texels (capped at 64) from

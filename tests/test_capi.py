@@ -55,6 +55,8 @@ def test_num_tiles_and_workspace_query():
     (dict(num_templates=0), "atlas"),
     (dict(t_stop=0.0), "t_stop"),
     (dict(atlas_kind=9), "atlas_kind"),
+    (dict(alpha_max=-0.5), "alpha_max"),
+    (dict(alpha_max=float("nan")), "alpha_max"),
 ])
 def test_invalid_canvas_is_rejected(bad, msg):
     from diffbmp_b200._lib import lib
