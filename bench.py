@@ -43,8 +43,8 @@ METRIC = "fwd+bwd iters/s at 2048^2 N=20k (FP16-storage fused vs plain FP32)"
 HEADLINE_KIND = "f16q"          # FP16 bilinear-quad atlas
 HEADLINE_KERNEL = "fused_kernel<32, F16_QUAD>"
 # DRAM bytes of one fused_kernel launch (FP16 quad atlas) on the 2048^2 / N=20k
-# scene, from one ncu capture (read 108.5 MB + write 3.8 MB); null for other configs.
-FUSED_DRAM_BYTES_C2 = 112.305e6
+# scene, from one ncu capture (read 108.0 MB + write 6.0 MB); null for other configs.
+FUSED_DRAM_BYTES_C2 = 114.029e6
 
 
 def parse():

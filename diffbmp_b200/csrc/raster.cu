@@ -823,12 +823,19 @@ struct TileWalker {
 // CTA shape of the walk kernels: a CTA runs kCtaWarps warps of one tile (the
 // warps walk independently, so a tile may be split over several CTAs, which
 // lets an SM refill as soon as a few warps finish); kParts CTAs per tile.
-// Registers are bounded for kWarpsPerSM resident warps per SM.
+// Registers are bounded for a number of resident warps per SM, tuned on B200
+// per atlas kind: 36 (56 registers a thread, a few bytes of spills) for the
+// packed atlases, whose walk waits mostly on texel loads and gains from the
+// extra warps; 32 (64 registers) for the reference layout and the
+// colour-map walks.
 #ifndef DBMP_CTA_WARPS
 #define DBMP_CTA_WARPS 4
 #endif
 #ifndef DBMP_WARPS_PER_SM
-#define DBMP_WARPS_PER_SM 32
+#define DBMP_WARPS_PER_SM 36
+#endif
+#ifndef DBMP_WARPS_PER_SM_F32
+#define DBMP_WARPS_PER_SM_F32 32
 #endif
 template <int TS> constexpr int kTileWarps() { return Layout<TS, DefaultNP<TS>::v>::NW; }
 template <int TS> constexpr int kCtaWarps() {
@@ -836,13 +843,14 @@ template <int TS> constexpr int kCtaWarps() {
 }
 template <int TS> constexpr int kParts() { return kTileWarps<TS>() / kCtaWarps<TS>(); }
 template <int TS> constexpr int kThreadsOf() { return kCtaWarps<TS>() * 32; }
-template <int TS> constexpr int kBlocksPerSM() {
-  return DBMP_WARPS_PER_SM / kCtaWarps<TS>() > 0 ? DBMP_WARPS_PER_SM / kCtaWarps<TS>() : 1;
+template <int TS, int KIND, bool CB = false> constexpr int kBlocksPerSM() {
+  constexpr int w = (KIND == ATLAS_F32 || CB) ? DBMP_WARPS_PER_SM_F32 : DBMP_WARPS_PER_SM;
+  return w / kCtaWarps<TS>() > 0 ? w / kCtaWarps<TS>() : 1;
 }
 
 // ---------------------------------------------------------------------------
 template <int TS, int KIND, bool CB>
-__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) forward_kernel(
+__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS, KIND, CB>()) forward_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, float* __restrict__ out_color, float* __restrict__ out_alpha,
     float* __restrict__ T_last, int* __restrict__ last_pos, const float* __restrict__ cmap, float cblend) {
@@ -891,7 +899,7 @@ __global__ void __launch_bounds__(kThreadsOf<TS>()) count_kernel(Geom g, const P
 }
 
 template <int TS, int KIND, bool CB>
-__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) backward_kernel(
+__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS, KIND, CB>()) backward_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, const float* __restrict__ T_last, const int* __restrict__ last_pos,
     const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc,
@@ -972,7 +980,7 @@ __global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const f
 // each warp leaves its partial in shared memory and the CTA's last warp to
 // finish its forward walk adds the CTA's sum (no barrier between the walks).
 template <int TS, int KIND>
-__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS>()) fused_kernel(
+__global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS, KIND>()) fused_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, const float* __restrict__ target, const float* __restrict__ background,
     float* __restrict__ out_image, double* __restrict__ gacc, double* __restrict__ loss_out,
