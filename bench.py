@@ -468,6 +468,12 @@ def main():
         "clocks": clocks,
     }
     if args.serving_jobs > 0 and world == 1:   # the serving stream is a single-GPU measurement
+        # measured on a clean device: the jobs above and their graphs are released first
+        for j in (job, plain, fused32, pair, e2e_job):
+            j.graph = None
+        del job, plain, fused32, pair, e2e_job, dev_params
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
         line["serving"] = run_serving(args.serving_jobs, rank, torch)
     if rank == 0 and world == 1 and not args.fast:
         ref = CpuReference(spec)
