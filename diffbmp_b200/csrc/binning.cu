@@ -179,7 +179,7 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
   pi.cg = sigmoid_precise(colors[3 * n + 1]);
   pi.cb = sigmoid_precise(colors[3 * n + 2]);
   const bool nan_geom = isnan(pi.a00) || isnan(pi.a01) || isnan(pi.a10) || isnan(pi.a11) || isnan(mx) || isnan(my);
-  pi.toff = !valid ? kNoFrag : (nan_geom ? kSolid : tid * template_records(g.kind, g.Ht, g.Wt));
+  pi.toff = (!valid || nan_geom) ? kNoFrag : tid * template_records(g.kind, g.Ht, g.Wt);
   // clearance a warp footprint needs before the walk may skip it: the
   // footprint's texel-space half extent, plus the bilinear reach of 1 texel,
   // plus slack for the rounding of the per-pixel texel coordinates

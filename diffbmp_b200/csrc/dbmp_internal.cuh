@@ -21,20 +21,21 @@ struct __align__(16) PrimInfo {
   float mx, my, hw, hh;      // centre, square-cull half extents (tile_forward.cu:194-210)
   float a00, a01, a10, a11;  // inverse affine to texel coordinates
   float alpha0, cr, cg, cb;  // alpha_max*sigmoid(opacity), sigmoid(colour logits)
-  int toff;                  // first element of the template in the atlas; kNoFrag / kSolid
+  int toff;                  // first element of the template in the atlas, or kNoFrag
   int goff;                  // first cell of the template's clearance grid (packed atlases)
   int gext;                  // clearance a warp footprint needs to be skipped (> kGridCap: never)
   int pad;
 };
 static_assert(sizeof(PrimInfo) == 64, "PrimInfo must be 64 bytes");
 
-// toff sentinels.  kNoFrag: invalid template id, the primitive never yields a
-// fragment (tile_forward.cu:211-216,274).  kSolid: NaN geometry; the
-// reference's range test lets NaN texel coordinates through, reads texel 0
-// and clamps the NaN mask to 1 (tile_common.h:177-197 + tile_forward.cu:271),
-// i.e. the primitive is opaque-by-mask wherever its cull passes.
+// toff sentinel kNoFrag: the primitive never yields a fragment.  Set for an
+// invalid template id (tile_forward.cu:211-216,274) and for NaN geometry (a NaN
+// centre, or a NaN in the inverse affine from a NaN or infinite rotation).  For
+// NaN geometry this is what the reference kernel computes as built with its
+// own flags (--use_fast_math): run side by side, no such primitive changes its
+// image, although its source, read literally, would clamp a NaN mask to 1
+// (tile_common.h:177-197, tile_forward.cu:271).
 constexpr int kNoFrag = -1;
-constexpr int kSolid = -2;
 
 // Texel storage of the template atlas.
 enum AtlasKind : int {

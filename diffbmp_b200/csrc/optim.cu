@@ -43,8 +43,11 @@ __global__ void adam_kernel(Geom g, AdamArgs a, const double* __restrict__ gacc,
   const double a0 = (double)g.alpha_max * sv;
   const double hx = g.hx, hy = g.hy;
   double grad[8];
-  grad[0] = a0 * rinv * (-c * hx * S[0] + s * hy * S[1]);
-  grad[1] = a0 * rinv * (-s * hx * S[0] - c * hy * S[1]);
+  // zero sums give zero gradients also for a non-finite rotation (see finalize_kernel)
+  const double cx = S[0] != 0.0 ? c * hx * S[0] : 0.0, sx = S[0] != 0.0 ? s * hx * S[0] : 0.0;
+  const double cy = S[1] != 0.0 ? c * hy * S[1] : 0.0, sy = S[1] != 0.0 ? s * hy * S[1] : 0.0;
+  grad[0] = a0 * rinv * (sy - cx);
+  grad[1] = a0 * rinv * (-sx - cy);
   grad[2] = -a0 * rinv * S[2];
   grad[3] = a0 * S[3];
   grad[4] = (1.0 - sv) * S[7];

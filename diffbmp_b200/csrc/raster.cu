@@ -357,12 +357,12 @@ struct TileWalker {
           const int toff = __float_as_int(q.x);
           if (toff != kNoFrag) {
             const float4 g1 = __ldg(r + 1);
-            if (kGrid && toff != kSolid)
+            if (kGrid)
               clear = grid_clear(g, grid, g0, g1, __float_as_int(q.y), __float_as_int(q.z), fcx, fcy);
             keep = KEEP_CLEAR || !clear;
             if (keep) {
               inside = footprint_inside(g0, fx0, fx1, fy0, fy1);
-              if (inside && toff != kSolid) {
+              if (inside) {
                 // texel box of the footprint: centre +- |A| (half extents), plus
                 // 0.05 texel for the rounding of the per-pixel coordinates
                 const float dx = fcx - g0.x, dy = fcy - g0.y;
@@ -450,23 +450,12 @@ struct TileWalker {
         const float4 c1 = w[e][3];
         const int toff = rec_toff(w[e]);
         const int pos = base - start + e;
-        float2 m;
-        bool ok0, ok1;
-        if (toff != kSolid) {
-          PairSample s;
-          const bool inside = (cm.inside >> e) & 1u;
-          if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
-          else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
-          m = pair_blend<false>(g, s, nullptr, nullptr);
-          ok0 = s.ok0;
-          ok1 = s.ok1;
-        } else {
-          // NaN geometry: every live pixel that passes the cull gets mask 1
-          ok0 = live[0] && !(fabsf(pxf[0] - g0.x) > g0.z || fabsf(pyf[0] - g0.y) > g0.w);
-          ok1 = live[1] && !(fabsf(pxf[1] - g0.x) > g0.z || fabsf(pyf[1] - g0.y) > g0.w);
-          m = make_float2(1.f, 1.f);
-        }
-        const bool f0 = ok0 && m.x > 1e-6f, f1 = ok1 && m.y > 1e-6f;
+        PairSample s;
+        const bool inside = (cm.inside >> e) & 1u;
+        if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+        else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+        const float2 m = pair_blend<false>(g, s, nullptr, nullptr);
+        const bool f0 = s.ok0 && m.x > 1e-6f, f1 = s.ok1 && m.y > 1e-6f;
         float2 a = mul2(make_float2(c0.x, c0.y), m);
         a.x = f0 ? a.x : 0.f;
         a.y = f1 ? a.y : 0.f;
@@ -522,28 +511,14 @@ struct TileWalker {
         const float4 c1 = w[e][3];
         const int toff = rec_toff(w[e]);
         const bool live[2] = {pos <= lp[0], pos <= lp[1]};
-        float2 m, gx, gy, tx, ty;
-        bool ok0, ok1;
-        if (toff != kSolid) {
-          PairSample s;
-          const bool inside = (cm.inside >> e) & 1u;
-          if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
-          else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
-          m = pair_blend<true>(g, s, &gx, &gy);
-          tx = s.tx;
-          ty = s.ty;
-          ok0 = s.ok0;
-          ok1 = s.ok1;
-        } else {
-          const float dx0 = pxf[0] - g0.x, dy0 = pyf[0] - g0.y, dx1 = pxf[1] - g0.x, dy1 = pyf[1] - g0.y;
-          ok0 = live[0] && !(fabsf(dx0) > g0.z || fabsf(dy0) > g0.w);
-          ok1 = live[1] && !(fabsf(dx1) > g0.z || fabsf(dy1) > g0.w);
-          tx = make_float2(fmaf(g1.x, dx0, fmaf(g1.y, dy0, g.hx)), fmaf(g1.x, dx1, fmaf(g1.y, dy1, g.hx)));
-          ty = make_float2(fmaf(g1.z, dx0, fmaf(g1.w, dy0, g.hy)), fmaf(g1.z, dx1, fmaf(g1.w, dy1, g.hy)));
-          m = make_float2(1.f, 1.f);
-          gx = gy = make_float2(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000));
-        }
-        const bool f0 = ok0 && m.x > 1e-6f, f1 = ok1 && m.y > 1e-6f;
+        PairSample s;
+        const bool inside = (cm.inside >> e) & 1u;
+        if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+        else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
+        float2 gx, gy;
+        const float2 m = pair_blend<true>(g, s, &gx, &gy);
+        const float2 tx = s.tx, ty = s.ty;
+        const bool f0 = s.ok0 && m.x > 1e-6f, f1 = s.ok1 && m.y > 1e-6f;
         float2 a = mul2(make_float2(c0.x, c0.y), m);
         a.x = f0 ? a.x : 0.f;
         a.y = f1 ? a.y : 0.f;
@@ -639,24 +614,14 @@ struct TileWalker {
         }
         Sample s[NP];
         float m[NP];
-        if (toff != kSolid) {
-          entry_sample<NP, L, KIND>(g, atlas, toff, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf,
-                                    live, s);
+        entry_sample<NP, L, KIND>(g, atlas, toff, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf,
+                                  live, s);
 #pragma unroll
-          for (int p = 0; p < NP; ++p) {
-            m[p] = blend<false>(s[p], nullptr, nullptr);
-            if (STATS) {
-              const bool c = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
-              n_cand += c;
-            }
-          }
-        } else {
-          // NaN geometry: every live pixel that passes the cull gets mask 1
-#pragma unroll
-          for (int p = 0; p < NP; ++p) {
-            s[p].ok = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
-            m[p] = 1.f;
-            if (STATS) n_cand += s[p].ok;
+        for (int p = 0; p < NP; ++p) {
+          m[p] = blend<false>(s[p], nullptr, nullptr);
+          if (STATS) {
+            const bool c = live[p] && !(fabsf(pxf[p] - g0.x) > g0.z || fabsf(pyf[p] - g0.y) > g0.w);
+            n_cand += c;
           }
         }
         if (STATS) {
@@ -766,22 +731,10 @@ struct TileWalker {
         for (int p = 0; p < NP; ++p) live[p] = pos <= lp[p];
         Sample s[NP];
         float m[NP], gx[NP], gy[NP];
-        if (toff != kSolid) {
-          entry_sample<NP, L, KIND>(g, atlas, toff, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf,
-                                    live, s);
+        entry_sample<NP, L, KIND>(g, atlas, toff, g0, g1, (cm.inside >> e) & 1u, (cm.fast >> e) & 1u, pxf, pyf,
+                                  live, s);
 #pragma unroll
-          for (int p = 0; p < NP; ++p) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
-        } else {
-#pragma unroll
-          for (int p = 0; p < NP; ++p) {
-            const float dx = pxf[p] - g0.x, dy = pyf[p] - g0.y;
-            s[p].ok = live[p] && !(fabsf(dx) > g0.z || fabsf(dy) > g0.w);
-            s[p].tx = fmaf(g1.x, dx, fmaf(g1.y, dy, g.hx));
-            s[p].ty = fmaf(g1.z, dx, fmaf(g1.w, dy, g.hy));
-            m[p] = 1.f;
-            gx[p] = gy[p] = __int_as_float(0x7fc00000);
-          }
-        }
+        for (int p = 0; p < NP; ++p) m[p] = blend<true>(s[p], &gx[p], &gy[p]);
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
           const bool frag = s[p].ok && m[p] > 1e-6f;
@@ -959,8 +912,13 @@ __global__ void finalize_kernel(Geom g, const float* __restrict__ radii, const f
   const double sv = sigmoid_d((double)opac[n]);
   const double a0 = (double)g.alpha_max * sv;
   const double hx = g.hx, hy = g.hy;
-  g_means[2 * n + 0] = (float)(a0 * rinv * (-c * hx * S[0] + s * hy * S[1]));
-  g_means[2 * n + 1] = (float)(a0 * rinv * (-s * hx * S[0] - c * hy * S[1]));
+  // A primitive without fragments has zero sums and zero gradients, also when
+  // its rotation is not finite (the reference adds gradients per fragment): a
+  // zero sum contributes 0 rather than NaN * 0.
+  const double cx = S[0] != 0.0 ? c * hx * S[0] : 0.0, sx = S[0] != 0.0 ? s * hx * S[0] : 0.0;
+  const double cy = S[1] != 0.0 ? c * hy * S[1] : 0.0, sy = S[1] != 0.0 ? s * hy * S[1] : 0.0;
+  g_means[2 * n + 0] = (float)(a0 * rinv * (sy - cx));
+  g_means[2 * n + 1] = (float)(a0 * rinv * (-sx - cy));
   g_radii[n] = (float)(-a0 * rinv * S[2]);
   g_rot[n] = (float)(a0 * S[3]);
   g_opac[n] = (float)((1.0 - sv) * S[7]);

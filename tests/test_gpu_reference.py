@@ -246,3 +246,73 @@ def test_colour_map_blend_vs_reference_kernel():
         spread = np.linalg.norm(hi[:, k] - lo[:, k]) / nrm
         print(f"  block {k}: reference vs FP64 {e_r:.2e}, ours vs reference {e_ro:.2e}, band {spread:.2e}")
         assert e_ro <= max(1e-4, 2 * e_r) + spread
+
+
+@pytest.mark.parametrize("kind", ["f32", "f16q"])
+@pytest.mark.parametrize("case", ["rot_nan", "rot_inf", "centre_nan"])
+def test_nan_geometry_vs_reference_kernel(kind, case):
+    """Primitives with NaN geometry (a NaN or infinite rotation, a NaN centre)
+    against the reference kernel built with its own flags (--use_fast_math,
+    oracle/Makefile): they yield no fragment there (its image equals the FP64
+    oracle, which drops non-finite texel coordinates), so ours must render the
+    same image and give them zero gradients; the other primitives' gradients
+    match the reference's."""
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.rasterizer import Atlas, Rasterizer
+    s = wl.make_scene("c0", 5)
+    th = np.array(s.rotations, np.float32)
+    m = np.array(s.means2D, np.float32)
+    nan_ids = np.array([3, 40, 200])
+    if case == "rot_nan":
+        th[nan_ids] = np.nan
+    elif case == "rot_inf":
+        th[nan_ids] = np.inf
+    else:
+        m[nan_ids, 0] = np.nan
+    sc = O.Scene(s.H, s.W, 32, m, s.radii, th, s.opacities, s.colors, s.templates, s.sel)
+    N, H, W = sc.N, sc.H, sc.W
+    offs, idx = bin_scene(sc)
+    rcol, ralp, rstate, fo = _run_reference(sc, offs, idx)
+    d, caches, counts, sig, K = rstate
+    rz = Rasterizer(H, W, 32, t_stop=1e-7)
+    atlas = Atlas(d["t"], kind)
+    _, lists = rz.bin(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], atlas)
+    assert np.array_equal(lists.mapping_tensor().cpu().numpy(), O.mapping_tensor(offs, idx))
+    # the NaN primitives are in the tile lists (binning lets NaN bounds through)
+    assert np.isin(nan_ids, idx).all()
+    col, alp, state = rz.forward(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], atlas)
+    torch.cuda.synchronize()
+    e_ref = np.abs(rcol.cpu().numpy() - fo["color"]).max()
+    band, _ = O.boundary_band(sc, offs, idx, edge=1e-3)
+    diff = np.maximum(np.abs(col.cpu().numpy() - rcol.cpu().numpy()).max(-1),
+                      np.abs(alp.cpu().numpy() - ralp.cpu().numpy()))
+    tol_f, tol_b = (max(2e-5, 2 * e_ref), 1e-3) if kind == "f32" else (3e-3, 2e-2)
+    print(case, kind, "reference vs FP64", e_ref, "ours vs reference outside band", diff[band == 0].max(initial=0))
+    assert diff[band == 0].max(initial=0) <= tol_f
+
+    rng = np.random.default_rng(5)
+    gc = rng.normal(0, 1, (H, W, 3)).astype(np.float32)
+    ga = rng.normal(0, 1, (H, W)).astype(np.float32)
+    t_gc, t_ga = dev(gc), dev(ga)
+    P, Ht, Wt = sc.templates.shape
+    rg = [torch.zeros(sh, device="cuda") for sh in ((N, 2), (N,), (N,), (N,), (N, 3))]
+    rc = RG.raster().ref_backward(H, W, 32, ctypes.c_float(1.0), N, P, Ht, Wt, K, P_(d["m"]), P_(d["r"]),
+                                  P_(d["th"]), P_(d["v"]), P_(d["c"]), P_(d["t"]), P_(d["s"]), P_(d["o"]), len(offs),
+                                  P_(d["i"]), len(idx), P_(t_gc), P_(t_ga), P_(caches), P_(counts), P_(sig),
+                                  *[P_(t) for t in rg])
+    assert rc == 0
+    ours = rz.backward(state, t_gc, t_ga, d["r"], d["th"], d["v"], d["c"], atlas)
+    rgn = np.concatenate([t.cpu().numpy().reshape(N, -1) for t in rg], 1)
+    ogn = np.concatenate([t.cpu().numpy().reshape(N, -1) for t in ours], 1)
+    # columns: centre x, y, radius, rotation, opacity, colour r, g, b
+    assert np.array_equal(rgn[nan_ids], np.zeros_like(rgn[nan_ids]))
+    assert np.array_equal(ogn[nan_ids], np.zeros_like(ogn[nan_ids]))
+    assert np.isfinite(ogn).all()
+    for k in range(8):
+        nrm = np.linalg.norm(rgn[:, k])
+        e = np.linalg.norm(ogn[:, k] - rgn[:, k]) / max(nrm, 1e-30)
+        print(f"  column {k}: ours vs reference {e:.2e}")
+        # c0's soft disk is rotationally symmetric, so dL/drotation is nearly 0
+        # and FP16 storage dominates its relative error (FP16 against FP32
+        # gradients: test_storage_kinds_track_fp32_gpu)
+        assert e <= (0.1 if (kind == "f16q" and k == 3) else tol_b)
