@@ -12,7 +12,8 @@ HBM; the plain FP32 kernels (unfused forward / backward, FP32 atlas in the
 reference layout) and the FP16 pair-layout atlas are timed beside it on the
 same scene.  ``e2e`` is the same iteration through the public Python API with the
 primitive parameters uploaded from pinned host memory before each step and
-the loss read back after it.  Multi-GPU (torchrun): every rank fits its own
+each step's loss read back by the host (one step in flight: the host reads
+step k-1's loss while step k runs).  Multi-GPU (torchrun): every rank fits its own
 independent job (replicas, no collective on the data path); value sums the
 ranks' iterations over the slowest rank's time.
 
@@ -43,8 +44,8 @@ METRIC = "fwd+bwd iters/s at 2048^2 N=20k (FP16-storage fused vs plain FP32)"
 HEADLINE_KIND = "f16q"          # FP16 bilinear-quad atlas
 HEADLINE_KERNEL = "fused_kernel<32, F16_QUAD>"
 # DRAM bytes of one fused_kernel launch (FP16 quad atlas) on the 2048^2 / N=20k
-# scene, from one ncu capture (read 108.0 MB + write 6.0 MB); null for other configs.
-FUSED_DRAM_BYTES_C2 = 114.029e6
+# scene, from one ncu capture (read 108.0 MB + write 3.6 MB); null for other configs.
+FUSED_DRAM_BYTES_C2 = 111.627e6
 
 
 def parse():
@@ -390,24 +391,38 @@ def main():
     e2e_job = build_job(spec, HEADLINE_KIND, True, torch)
     host = {k: torch.from_numpy(np.ascontiguousarray(getattr(spec, k), np.float32)).pin_memory()
             for k in ("means2D", "radii", "rotations", "opacities", "colors")}
-    loss_host = torch.zeros(1, dtype=torch.float64).pin_memory()
+    loss_host = torch.zeros(2, dtype=torch.float64).pin_memory()   # ring of two step results
+    done = [torch.cuda.Event(), torch.cuda.Event()]
     dev_params = e2e_job.params()
     h2d = sum(v.numel() * 4 for v in host.values())
+    losses = []
 
-    def e2e_step():
+    def e2e_step(i):
+        # one step in flight: step i is enqueued (inputs H2D, iteration, loss
+        # D2H), then the host waits for step i - 1 and reads its loss
         for k, v in host.items():
             dev_params[k].copy_(v.view_as(dev_params[k]), non_blocking=True)
         e2e_job.step()
-        loss_host.copy_(e2e_job.loss_dev, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
-    for _ in range(args.warmup):
-        e2e_step()
+        loss_host[i % 2:i % 2 + 1].copy_(e2e_job.loss_dev, non_blocking=True)
+        done[i % 2].record()
+        if i > 0:
+            done[(i - 1) % 2].synchronize()
+            losses.append(float(loss_host[(i - 1) % 2]))
+
+    def e2e_finish(n):
+        done[(n - 1) % 2].synchronize()
+        losses.append(float(loss_host[(n - 1) % 2]))
+    for i in range(args.warmup):
+        e2e_step(i)
+    e2e_finish(args.warmup)
     e2e_job.sync()
     torch.cuda.synchronize(); barrier(world)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
+    for i in range(args.steps):
+        e2e_step(i)
+    e2e_finish(args.steps)
     t_e2e = time.perf_counter() - t0
+    assert len(losses) == args.warmup + args.steps and all(np.isfinite(losses))
     t_e2e = max_over_ranks(t_e2e, world)
 
     # --- roofline of the dominant kernel (fused fwd+bwd), CUDA events ------
@@ -461,7 +476,8 @@ def main():
                      "hbm_peak_gbs_measured": peaks.get("hbm_gbs")},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 8,
-                "what": "public API: params H2D from pinned host, ImageFitter.step(), loss D2H, synchronised"},
+                "what": "public API: params H2D from pinned host, ImageFitter.step(), loss D2H read by the host "
+                        "every step, one step in flight"},
         "gpu_launches": 6 * args.steps,
         "gpu_launches_note": "ours per step: prepare, counts, bin_rows, fused, adam, step_increment "
                              "(+ one memset and the two kernels of one CUB exclusive scan over the tile counts)",

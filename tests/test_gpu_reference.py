@@ -316,3 +316,25 @@ def test_nan_geometry_vs_reference_kernel(kind, case):
         # and FP16 storage dominates its relative error (FP16 against FP32
         # gradients: test_storage_kinds_track_fp32_gpu)
         assert e <= (0.1 if (kind == "f16q" and k == 3) else tol_b)
+
+
+def test_alpha_above_one_forward_vs_reference_kernel():
+    """alpha_max > 1: fragments with alpha > 1 zero the transmittance, as the
+    reference's T *= max(1 - a, 0) (tile_forward.cu:390) does."""
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.rasterizer import Atlas, Rasterizer
+    s = wl.make_scene("c0", 6)
+    sc = O.Scene(s.H, s.W, 32, s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.templates, s.sel, 1.5)
+    offs, idx = bin_scene(sc)
+    rcol, ralp, rstate, fo = _run_reference(sc, offs, idx)
+    d = rstate[0]
+    rz = Rasterizer(sc.H, sc.W, 32, alpha_max=1.5, t_stop=1e-7)
+    for kind in ("f32", "f16q"):
+        col, alp, _ = rz.forward(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], Atlas(d["t"], kind))
+        torch.cuda.synchronize()
+        e_ref = np.abs(rcol.cpu().numpy() - fo["color"]).max()
+        band, _ = O.boundary_band(sc, offs, idx, edge=1e-3)
+        diff = np.maximum(np.abs(col.cpu().numpy() - rcol.cpu().numpy()).max(-1),
+                          np.abs(alp.cpu().numpy() - ralp.cpu().numpy()))
+        print(kind, "reference vs FP64", e_ref, "ours vs reference outside band", diff[band == 0].max(initial=0))
+        assert diff[band == 0].max(initial=0) <= (max(2e-5, 2 * e_ref) if kind == "f32" else 3e-3)
