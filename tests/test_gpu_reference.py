@@ -249,9 +249,10 @@ def test_colour_map_blend_vs_reference_kernel():
 
 
 @pytest.mark.parametrize("kind", ["f32", "f16q"])
-@pytest.mark.parametrize("case", ["rot_nan", "rot_inf", "centre_nan"])
+@pytest.mark.parametrize("case", ["rot_nan", "rot_inf", "centre_nan", "radius_tiny", "radius_zero", "radius_neg"])
 def test_nan_geometry_vs_reference_kernel(kind, case):
     """Primitives with NaN geometry (a NaN or infinite rotation, a NaN centre)
+    or a degenerate radius (below the reference's 1e-6 floor, zero, negative)
     against the reference kernel built with its own flags (--use_fast_math,
     oracle/Makefile): they yield no fragment there (its image equals the FP64
     oracle, which drops non-finite texel coordinates), so ours must render the
@@ -263,13 +264,16 @@ def test_nan_geometry_vs_reference_kernel(kind, case):
     th = np.array(s.rotations, np.float32)
     m = np.array(s.means2D, np.float32)
     nan_ids = np.array([3, 40, 200])
+    r = np.array(s.radii, np.float32)
     if case == "rot_nan":
         th[nan_ids] = np.nan
     elif case == "rot_inf":
         th[nan_ids] = np.inf
-    else:
+    elif case == "centre_nan":
         m[nan_ids, 0] = np.nan
-    sc = O.Scene(s.H, s.W, 32, m, s.radii, th, s.opacities, s.colors, s.templates, s.sel)
+    else:
+        r[nan_ids] = {"radius_tiny": 5e-7, "radius_zero": 0.0, "radius_neg": -20.0}[case]
+    sc = O.Scene(s.H, s.W, 32, m, r, th, s.opacities, s.colors, s.templates, s.sel)
     N, H, W = sc.N, sc.H, sc.W
     offs, idx = bin_scene(sc)
     rcol, ralp, rstate, fo = _run_reference(sc, offs, idx)
@@ -278,8 +282,9 @@ def test_nan_geometry_vs_reference_kernel(kind, case):
     atlas = Atlas(d["t"], kind)
     _, lists = rz.bin(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], atlas)
     assert np.array_equal(lists.mapping_tensor().cpu().numpy(), O.mapping_tensor(offs, idx))
-    # the NaN primitives are in the tile lists (binning lets NaN bounds through)
-    assert np.isin(nan_ids, idx).all()
+    if case in ("rot_nan", "rot_inf", "centre_nan"):
+        # the NaN primitives are in the tile lists (binning lets NaN bounds through)
+        assert np.isin(nan_ids, idx).all()
     col, alp, state = rz.forward(d["m"], d["r"], d["th"], d["v"], d["c"], d["s"], atlas)
     torch.cuda.synchronize()
     e_ref = np.abs(rcol.cpu().numpy() - fo["color"]).max()
