@@ -153,6 +153,7 @@ struct Quad { float v00, d01, v10, d11; };
 template <int KIND> struct AtlasFetch;
 
 template <> struct AtlasFetch<ATLAS_F32> {
+  using Raw = float4;
   // the four neighbours as loaded: (v00, v01, v10, v11)
   static __device__ __forceinline__ float4 get_raw(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     const float* t = static_cast<const float*>(atlas) + off + y0 * Wt + x0;
@@ -166,13 +167,17 @@ template <> struct AtlasFetch<ATLAS_F32> {
   }
 };
 
+// Packed kinds: load() fetches record i (= off + y0 Wt + x0; int or unsigned)
+// as stored, unpack() turns it into a Quad, at() does both.
 template <> struct AtlasFetch<ATLAS_F32_QUAD> {
-  // record i (= off + y0 Wt + x0; int or unsigned)
+  using Raw = float4;
   template <typename I>
-  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
-    const float4 v = __ldg(static_cast<const float4*>(atlas) + i);
-    return Quad{v.x, v.y, v.z, v.w};
+  static __device__ __forceinline__ Raw load(const void* atlas, I i, int Wt) {
+    return __ldg(static_cast<const float4*>(atlas) + i);
   }
+  static __device__ __forceinline__ Quad unpack(const Raw& v) { return Quad{v.x, v.y, v.z, v.w}; }
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) { return unpack(load(atlas, i, Wt)); }
   static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     return at(atlas, off + y0 * Wt + x0, Wt);
   }
@@ -184,48 +189,70 @@ __device__ __forceinline__ float2 b2f(unsigned u) {
 }
 
 template <> struct AtlasFetch<ATLAS_F16_QUAD> {
+  using Raw = uint2;
   template <typename I>
-  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
-    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + i);
-    const float2 a = h2f(raw.x), b = h2f(raw.y);
+  static __device__ __forceinline__ Raw load(const void* atlas, I i, int Wt) {
+    return __ldg(static_cast<const uint2*>(atlas) + i);
+  }
+  static __device__ __forceinline__ Quad unpack(const Raw& r) {
+    const float2 a = h2f(r.x), b = h2f(r.y);
     return Quad{a.x, a.y, b.x, b.y};
   }
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) { return unpack(load(atlas, i, Wt)); }
   static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
 template <> struct AtlasFetch<ATLAS_BF16_QUAD> {
+  using Raw = uint2;
   template <typename I>
-  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
-    const uint2 raw = __ldg(static_cast<const uint2*>(atlas) + i);
-    const float2 a = b2f(raw.x), b = b2f(raw.y);
+  static __device__ __forceinline__ Raw load(const void* atlas, I i, int Wt) {
+    return __ldg(static_cast<const uint2*>(atlas) + i);
+  }
+  static __device__ __forceinline__ Quad unpack(const Raw& r) {
+    const float2 a = b2f(r.x), b = b2f(r.y);
     return Quad{a.x, a.y, b.x, b.y};
   }
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) { return unpack(load(atlas, i, Wt)); }
   static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
 template <> struct AtlasFetch<ATLAS_F16_PAIR> {
+  using Raw = uint2;   // (record i, record i + Wt): rows y and y + 1; row Ht is the zero pad
   template <typename I>
-  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+  static __device__ __forceinline__ Raw load(const void* atlas, I i, int Wt) {
     const unsigned* p = static_cast<const unsigned*>(atlas) + i;
-    const float2 a = h2f(__ldg(p)), b = h2f(__ldg(p + Wt));   // row Ht is the zero pad
+    return make_uint2(__ldg(p), __ldg(p + Wt));
+  }
+  static __device__ __forceinline__ Quad unpack(const Raw& r) {
+    const float2 a = h2f(r.x), b = h2f(r.y);
     return Quad{a.x, a.y, b.x, b.y};
   }
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) { return unpack(load(atlas, i, Wt)); }
   static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     return at(atlas, off + y0 * Wt + x0, Wt);
   }
 };
 
 template <> struct AtlasFetch<ATLAS_BF16_PAIR> {
+  using Raw = uint2;
   template <typename I>
-  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) {
+  static __device__ __forceinline__ Raw load(const void* atlas, I i, int Wt) {
     const unsigned* p = static_cast<const unsigned*>(atlas) + i;
-    const float2 a = b2f(__ldg(p)), b = b2f(__ldg(p + Wt));
+    return make_uint2(__ldg(p), __ldg(p + Wt));
+  }
+  static __device__ __forceinline__ Quad unpack(const Raw& r) {
+    const float2 a = b2f(r.x), b = b2f(r.y);
     return Quad{a.x, a.y, b.x, b.y};
   }
+  template <typename I>
+  static __device__ __forceinline__ Quad at(const void* atlas, I i, int Wt) { return unpack(load(atlas, i, Wt)); }
   static __device__ __forceinline__ Quad get(const void* atlas, int off, int Ht, int Wt, int x0, int y0) {
     return at(atlas, off + y0 * Wt + x0, Wt);
   }

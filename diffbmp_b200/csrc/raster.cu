@@ -163,46 +163,83 @@ struct PairSample {
   bool ok0, ok1;             // pixel can yield a fragment (as Sample::ok)
 };
 
+// A pixel pair's sample with its texel loads issued but not yet consumed.
+template <int KIND>
+struct PairPre {
+  float2 wx, wy;
+  typename AtlasFetch<KIND>::Raw r0, r1;   // the two pixels' records as loaded
+  bool ok0, ok1;
+};
+
+// Coordinates, weights and texel loads of both pixels for one entry; tx, ty
+// (optional) receive the texel coordinates.
 template <class L, int KIND, bool FAST>
-__device__ __forceinline__ void pair_sample(const Geom& g, const void* __restrict__ atlas, int toff,
-                                            const float4& g0, const float4& g1, bool inside, const float (&pxf)[2],
-                                            const float (&pyf)[2], const bool (&live)[2], PairSample& s) {
+__device__ __forceinline__ void pair_prep(const Geom& g, const void* __restrict__ atlas, int toff,
+                                          const float4& g0, const float4& g1, bool inside, const float (&pxf)[2],
+                                          const float (&pyf)[2], const bool (&live)[2], PairPre<KIND>& s,
+                                          float2* ptx = nullptr, float2* pty = nullptr) {
   Sample c[2];
   entry_coords<2, L, FAST>(g, g0, g1, inside, pxf, pyf, live, c);
   s.ok0 = c[0].ok;
   s.ok1 = c[1].ok;
-  s.tx = make_float2(c[0].tx, c[1].tx);
-  s.ty = make_float2(c[0].ty, c[1].ty);
+  if (ptx) {
+    *ptx = make_float2(c[0].tx, c[1].tx);
+    *pty = make_float2(c[0].ty, c[1].ty);
+  }
   // pixels without a fragment sample texel 0 of the template (in bounds)
-  const float2 tx = FAST ? s.tx : make_float2(c[0].ok ? c[0].tx : 0.f, c[1].ok ? c[1].tx : 0.f);
-  const float2 ty = FAST ? s.ty : make_float2(c[0].ok ? c[0].ty : 0.f, c[1].ok ? c[1].ty : 0.f);
+  const float2 tx = make_float2((FAST || c[0].ok) ? c[0].tx : 0.f, (FAST || c[1].ok) ? c[1].tx : 0.f);
+  const float2 ty = make_float2((FAST || c[0].ok) ? c[0].ty : 0.f, (FAST || c[1].ok) ? c[1].ty : 0.f);
   // floor as in floor_small: adding 2^23 rounding toward zero
   const float2 bx = __fadd2_rz(tx, g.k23), by = __fadd2_rz(ty, g.k23);
   const float2 fx = fma2(g.m1, g.k23, bx), fy = fma2(g.m1, g.k23, by);
   s.wx = sub2(g, tx, fx);
   s.wy = sub2(g, ty, fy);
   if constexpr (KIND == ATLAS_F32) {
-    // reference layout: both pixels' differences as packed subtractions
     const int x0 = __float_as_int(bx.x) - 0x4B000000, y0 = __float_as_int(by.x) - 0x4B000000;
     const int x1 = __float_as_int(bx.y) - 0x4B000000, y1 = __float_as_int(by.y) - 0x4B000000;
-    const float4 r0 = AtlasFetch<KIND>::get_raw(atlas, toff, g.Ht, g.Wt, x0, y0);
-    const float4 r1 = AtlasFetch<KIND>::get_raw(atlas, toff, g.Ht, g.Wt, x1, y1);
-    s.v00 = make_float2(r0.x, r1.x);
-    s.v10 = make_float2(r0.z, r1.z);
-    s.d01 = sub2(g, make_float2(r0.y, r1.y), s.v00);
-    s.d11 = sub2(g, make_float2(r0.w, r1.w), s.v10);
+    s.r0 = AtlasFetch<KIND>::get_raw(atlas, toff, g.Ht, g.Wt, x0, y0);
+    s.r1 = AtlasFetch<KIND>::get_raw(atlas, toff, g.Ht, g.Wt, x1, y1);
   } else {
     // record index toff + y0 Wt + x0 straight from the biased bit patterns
     // (2^23 + x0, 2^23 + y0): the bias is one constant per entry, and the
     // unsigned arithmetic wraps back to the in-range index
     const unsigned c = (unsigned)toff - g.kbias;
-    const Quad q0 = AtlasFetch<KIND>::at(atlas, __float_as_uint(by.x) * (unsigned)g.Wt + __float_as_uint(bx.x) + c, g.Wt);
-    const Quad q1 = AtlasFetch<KIND>::at(atlas, __float_as_uint(by.y) * (unsigned)g.Wt + __float_as_uint(bx.y) + c, g.Wt);
+    s.r0 = AtlasFetch<KIND>::load(atlas, __float_as_uint(by.x) * (unsigned)g.Wt + __float_as_uint(bx.x) + c, g.Wt);
+    s.r1 = AtlasFetch<KIND>::load(atlas, __float_as_uint(by.y) * (unsigned)g.Wt + __float_as_uint(bx.y) + c, g.Wt);
+  }
+}
+
+// Consumes the loads of pair_prep: weights and neighbours as pairs (the
+// neighbours in difference form); tx, ty are not set.
+template <int KIND>
+__device__ __forceinline__ void pair_unpack(const Geom& g, const PairPre<KIND>& p, PairSample& s) {
+  s.wx = p.wx;
+  s.wy = p.wy;
+  s.ok0 = p.ok0;
+  s.ok1 = p.ok1;
+  if constexpr (KIND == ATLAS_F32) {
+    // reference layout: both pixels' differences as packed subtractions
+    s.v00 = make_float2(p.r0.x, p.r1.x);
+    s.v10 = make_float2(p.r0.z, p.r1.z);
+    s.d01 = sub2(g, make_float2(p.r0.y, p.r1.y), s.v00);
+    s.d11 = sub2(g, make_float2(p.r0.w, p.r1.w), s.v10);
+  } else {
+    const Quad q0 = AtlasFetch<KIND>::unpack(p.r0), q1 = AtlasFetch<KIND>::unpack(p.r1);
     s.v00 = make_float2(q0.v00, q1.v00);
     s.d01 = make_float2(q0.d01, q1.d01);
     s.v10 = make_float2(q0.v10, q1.v10);
     s.d11 = make_float2(q0.d11, q1.d11);
   }
+}
+
+// Both phases for one entry, with the texel coordinates.
+template <class L, int KIND, bool FAST>
+__device__ __forceinline__ void pair_sample(const Geom& g, const void* __restrict__ atlas, int toff,
+                                            const float4& g0, const float4& g1, bool inside, const float (&pxf)[2],
+                                            const float (&pyf)[2], const bool (&live)[2], PairSample& s) {
+  PairPre<KIND> p;
+  pair_prep<L, KIND, FAST>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, p, &s.tx, &s.ty);
+  pair_unpack<KIND>(g, p, s);
 }
 
 // Bilinear mask of both pixels (upper-clamped as in blend()) and, with GRAD, its texel-space
@@ -427,59 +464,91 @@ struct TileWalker {
     if (lane < 8 && acc[0] != 0.f) atomicAdd(dst + kidx, (double)acc[0]);
   }
 
+  // Phase 1 of a forward entry for a pixel pair: coordinates and texel loads.
+  __device__ __forceinline__ void pair_issue(const Geom& g, const void* __restrict__ atlas, const Rec* w, int e,
+                                             const ChunkMasks& cm, const bool (&live)[2], PairPre<KIND>& p) const {
+    const int toff = rec_toff(w[e]);
+    const float4 g0 = w[e][0];
+    const float4 g1 = w[e][1];
+    const bool inside = (cm.inside >> e) & 1u;
+    if ((cm.fast >> e) & 1u) pair_prep<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, p);
+    else pair_prep<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, p);
+  }
+
+  // Forward state of a pixel pair.
+  struct PairFwd {
+    float2 cr, cg, cb, t, tl;
+    int lp0, lp1;
+    bool live[2];
+  };
+
+  // Phase 2 of a forward entry: blend the loaded texels and composite.
+  // Returns true when every pixel of the warp has stopped.
+  __device__ __forceinline__ bool pair_composite(const Geom& g, const Rec* w, int e, int pos, const PairPre<KIND>& p,
+                                                 PairFwd& f) const {
+    const float4 c0 = w[e][2];
+    const float4 c1 = w[e][3];
+    PairSample s;
+    pair_unpack<KIND>(g, p, s);
+    const float2 m = pair_blend<false>(g, s, nullptr, nullptr);
+    // a pixel may have stopped since the loads were issued
+    const bool f0 = s.ok0 && f.live[0] && m.x > 1e-6f, f1 = s.ok1 && f.live[1] && m.y > 1e-6f;
+    float2 a = mul2(make_float2(c0.x, c0.y), m);
+    a.x = f0 ? a.x : 0.f;
+    a.y = f1 ? a.y : 0.f;
+    const float2 wt = mul2(f.t, a);
+    f.cr = fma2(wt, make_float2(c0.z, c0.w), f.cr);
+    f.cg = fma2(wt, make_float2(c1.x, c1.y), f.cg);
+    f.cb = fma2(wt, make_float2(c1.z, c1.w), f.cb);
+    f.tl.x = f0 ? f.t.x : f.tl.x;
+    f.tl.y = f1 ? f.t.y : f.tl.y;
+    f.lp0 = f0 ? pos : f.lp0;
+    f.lp1 = f1 ? pos : f.lp1;
+    // T (1 - a) as in forward(), saturated per pixel (no packed form)
+    f.t.x = __saturatef(fmaf(-f.t.x, a.x, f.t.x));
+    f.t.y = __saturatef(fmaf(-f.t.y, a.y, f.t.y));
+    f.live[0] = f.live[0] && !(f.t.x < g.t_stop);
+    f.live[1] = f.live[1] && !(f.t.y < g.t_stop);
+    return __all_sync(kFull, !f.live[0] && !f.live[1]);
+  }
+
   // Forward walk of the pixel-pair form: the walk of forward() with both
-  // pixels' sampling, blending and compositing as packed pairs.
+  // pixels' sampling, blending and compositing as packed pairs.  Entries go
+  // two at a time: the texel loads of both are issued before either is
+  // composited, so their latencies overlap.
   __device__ __forceinline__ void forward_pair(const Geom& g, const PrimInfo* __restrict__ prims,
                                                const void* __restrict__ atlas, const int* __restrict__ idx, Rec* w,
                                                float (&C)[2][3], float (&T)[2], float (&Tl)[2], int (&lp)[2]) {
     const unsigned char* grid = static_cast<const unsigned char*>(atlas) + g.grid_off;
-    bool live[2] = {valid[0], valid[1]};
-    float2 cr = make_float2(0.f, 0.f), cg = cr, cb = cr, t = make_float2(1.f, 1.f), tl = t;
-    int lp0 = -1, lp1 = -1;
-    bool warp_done = __all_sync(kFull, !live[0] && !live[1]);
+    PairFwd f;
+    f.cr = f.cg = f.cb = make_float2(0.f, 0.f);
+    f.t = f.tl = make_float2(1.f, 1.f);
+    f.lp0 = f.lp1 = -1;
+    f.live[0] = valid[0];
+    f.live[1] = valid[1];
+    bool warp_done = __all_sync(kFull, !f.live[0] && !f.live[1]);
     for (int base = start; base < end && !warp_done; base += kChunk) {
       int my_id;
       const ChunkMasks cm = stage<false>(g, prims, idx, grid, base, end, w, &my_id);
       unsigned todo = cm.todo;
       while (todo) {
-        const int e = __ffs(todo) - 1;
+        const int e1 = __ffs(todo) - 1;
         todo &= todo - 1;
-        const float4 g0 = w[e][0];
-        const float4 g1 = w[e][1];
-        const float4 c0 = w[e][2];
-        const float4 c1 = w[e][3];
-        const int toff = rec_toff(w[e]);
-        const int pos = base - start + e;
-        PairSample s;
-        const bool inside = (cm.inside >> e) & 1u;
-        if ((cm.fast >> e) & 1u) pair_sample<L, KIND, true>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
-        else pair_sample<L, KIND, false>(g, atlas, toff, g0, g1, inside, pxf, pyf, live, s);
-        const float2 m = pair_blend<false>(g, s, nullptr, nullptr);
-        const bool f0 = s.ok0 && m.x > 1e-6f, f1 = s.ok1 && m.y > 1e-6f;
-        float2 a = mul2(make_float2(c0.x, c0.y), m);
-        a.x = f0 ? a.x : 0.f;
-        a.y = f1 ? a.y : 0.f;
-        const float2 wt = mul2(t, a);
-        cr = fma2(wt, make_float2(c0.z, c0.w), cr);
-        cg = fma2(wt, make_float2(c1.x, c1.y), cg);
-        cb = fma2(wt, make_float2(c1.z, c1.w), cb);
-        tl.x = f0 ? t.x : tl.x;
-        tl.y = f1 ? t.y : tl.y;
-        lp0 = f0 ? pos : lp0;
-        lp1 = f1 ? pos : lp1;
-        // T (1 - a) as in forward(), saturated per pixel (no packed form)
-        t.x = __saturatef(fmaf(-t.x, a.x, t.x));
-        t.y = __saturatef(fmaf(-t.y, a.y, t.y));
-        live[0] = live[0] && !(t.x < g.t_stop);
-        live[1] = live[1] && !(t.y < g.t_stop);
-        if (__all_sync(kFull, !live[0] && !live[1])) { warp_done = true; break; }
+        const bool two = todo != 0;
+        const int e2 = two ? __ffs(todo) - 1 : e1;   // e1 again when it is the chunk's last
+        todo &= todo - 1;
+        PairPre<KIND> p1, p2;
+        pair_issue(g, atlas, w, e1, cm, f.live, p1);
+        pair_issue(g, atlas, w, e2, cm, f.live, p2);
+        if (pair_composite(g, w, e1, base - start + e1, p1, f)) { warp_done = true; break; }
+        if (two && pair_composite(g, w, e2, base - start + e2, p2, f)) { warp_done = true; break; }
       }
     }
-    C[0][0] = cr.x; C[0][1] = cg.x; C[0][2] = cb.x;
-    C[1][0] = cr.y; C[1][1] = cg.y; C[1][2] = cb.y;
-    T[0] = t.x; T[1] = t.y;
-    Tl[0] = tl.x; Tl[1] = tl.y;
-    lp[0] = lp0; lp[1] = lp1;
+    C[0][0] = f.cr.x; C[0][1] = f.cg.x; C[0][2] = f.cb.x;
+    C[1][0] = f.cr.y; C[1][1] = f.cg.y; C[1][2] = f.cb.y;
+    T[0] = f.t.x; T[1] = f.t.y;
+    Tl[0] = f.tl.x; Tl[1] = f.tl.y;
+    lp[0] = f.lp0; lp[1] = f.lp1;
   }
 
   // Reverse walk of the pixel-pair form (the walk of backward() with both
