@@ -44,8 +44,8 @@ METRIC = "fwd+bwd iters/s at 2048^2 N=20k (FP16-storage fused vs plain FP32)"
 HEADLINE_KIND = "f16q"          # FP16 bilinear-quad atlas
 HEADLINE_KERNEL = "fused_kernel<32, F16_QUAD>"
 # DRAM bytes of one fused_kernel launch (FP16 quad atlas) on the 2048^2 / N=20k
-# scene, from one ncu capture (read 108.0 MB + write 3.6 MB); null for other configs.
-FUSED_DRAM_BYTES_C2 = 111.627e6
+# scene, from one ncu capture (read 108.3 MB + write 3.8 MB); null for other configs.
+FUSED_DRAM_BYTES_C2 = 112.057e6
 
 
 def parse():
