@@ -16,7 +16,10 @@
 // 0 of the template, so every load is in bounds), then composites them
 // branch-free.  A warp stops when all its pixels are below t_stop; the
 // backward walk of a warp starts at its own last contributor and adds its
-// warp-reduced per-primitive sums straight into the FP64 accumulator.
+// warp-reduced per-primitive sums straight into the FP64 accumulator.  With 2
+// pixels per thread (32x32 tiles) both pixels go through the arithmetic as one
+// float2 of packed FP32x2 instructions, and the forward walk issues the
+// texel loads of two entries before compositing either.
 #include "dbmp_internal.cuh"
 
 namespace dbmp {
