@@ -151,7 +151,11 @@ __device__ __forceinline__ float blend(const Sample& s, float* gx, float* gy) {
 // pixels runs as one float2 (x: pixel 0, y: pixel 1) through the packed FP32x2
 // instructions of sm_100, one instruction for both pixels.  Each packed
 // operation rounds exactly like its scalar counterpart; constant operands come
-// as pairs from the kernel parameters (Geom) or the staged record.
+// as pairs from the kernel parameters (Geom) or the staged record.  Packed
+// operations issue to the FMA-heavy pipe only, while scalar FP32 operations
+// may also use the FMA-lite pipe, so some steps stay scalar to keep both pipes
+// busy (measured on B200: the forward's blend and colour accumulation, the
+// backward's colour and per-primitive product terms).
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
@@ -246,9 +250,20 @@ __device__ __forceinline__ void pair_sample(const Geom& g, const void* __restric
 }
 
 // Bilinear mask of both pixels (upper-clamped as in blend()) and, with GRAD, its texel-space
-// gradient: the operations of blend() on pairs.
-template <bool GRAD>
+// gradient: the operations of blend() on pairs.  PACKED: as FP32x2 instructions;
+// otherwise as scalar ones (same roundings).
+template <bool GRAD, bool PACKED = true>
 __device__ __forceinline__ float2 pair_blend(const Geom& g, const PairSample& s, float2* gx, float2* gy) {
+  if (!PACKED) {
+    const float top0 = fmaf(s.wx.x, s.d01.x, s.v00.x), top1 = fmaf(s.wx.y, s.d01.y, s.v00.y);
+    const float bot0 = fmaf(s.wx.x, s.d11.x, s.v10.x), bot1 = fmaf(s.wx.y, s.d11.y, s.v10.y);
+    const float d0 = bot0 - top0, d1 = bot1 - top1;
+    if (GRAD) {
+      *gx = make_float2(fmaf(s.wy.x, s.d11.x - s.d01.x, s.d01.x), fmaf(s.wy.y, s.d11.y - s.d01.y, s.d01.y));
+      *gy = make_float2(d0, d1);
+    }
+    return make_float2(fminf(1.f, fmaf(s.wy.x, d0, top0)), fminf(1.f, fmaf(s.wy.y, d1, top1)));
+  }
   const float2 dt = s.d01, db = s.d11;
   const float2 top = fma2(s.wx, dt, s.v00);
   const float2 bot = fma2(s.wx, db, s.v10);
@@ -493,16 +508,16 @@ struct TileWalker {
     const float4 c1 = w[e][3];
     PairSample s;
     pair_unpack<KIND>(g, p, s);
-    const float2 m = pair_blend<false>(g, s, nullptr, nullptr);
+    const float2 m = pair_blend<false, false>(g, s, nullptr, nullptr);
     // a pixel may have stopped since the loads were issued
     const bool f0 = s.ok0 && f.live[0] && m.x > 1e-6f, f1 = s.ok1 && f.live[1] && m.y > 1e-6f;
     float2 a = mul2(make_float2(c0.x, c0.y), m);
     a.x = f0 ? a.x : 0.f;
     a.y = f1 ? a.y : 0.f;
-    const float2 wt = mul2(f.t, a);
-    f.cr = fma2(wt, make_float2(c0.z, c0.w), f.cr);
-    f.cg = fma2(wt, make_float2(c1.x, c1.y), f.cg);
-    f.cb = fma2(wt, make_float2(c1.z, c1.w), f.cb);
+    const float2 wt = make_float2(f.t.x * a.x, f.t.y * a.y);
+    f.cr = make_float2(fmaf(wt.x, c0.z, f.cr.x), fmaf(wt.y, c0.w, f.cr.y));
+    f.cg = make_float2(fmaf(wt.x, c1.x, f.cg.x), fmaf(wt.y, c1.y, f.cg.y));
+    f.cb = make_float2(fmaf(wt.x, c1.z, f.cb.x), fmaf(wt.y, c1.w, f.cb.y));
     f.tl.x = f0 ? f.t.x : f.tl.x;
     f.tl.y = f1 ? f.t.y : f.tl.y;
     f.lp0 = f0 ? pos : f.lp0;
@@ -601,7 +616,8 @@ struct TileWalker {
         ts = tk;
         const float2 col_r = make_float2(c0.z, c0.w), col_g = make_float2(c1.x, c1.y),
                      col_b = make_float2(c1.z, c1.w);
-        const float2 gcc = fma2(gcr, col_r, fma2(gcg, col_g, mul2(gcb, col_b)));
+        const float2 gcc = make_float2(fmaf(gcr.x, col_r.x, fmaf(gcg.x, col_g.x, gcb.x * col_b.x)),
+                                       fmaf(gcr.y, col_r.y, fmaf(gcg.y, col_g.y, gcb.y * col_b.y)));
         const float2 dlda = mul2(tk, fma2(ga, bt, sub2(g, gcc, h)));
         const float2 u = mul2(dlda, make_float2(f0 ? gx.x : 0.f, f1 ? gx.y : 0.f));
         const float2 v = mul2(dlda, make_float2(f0 ? gy.x : 0.f, f1 ? gy.y : 0.f));
@@ -618,15 +634,12 @@ struct TileWalker {
           const float2 r = fma2(mul2(u, g.rxy2), ey, mul2(mul2(v, g.nryx2), ex));
           acc[3] = r.x + r.y;
         }
-        {
-          const float2 r4 = mul2(gcr, wt), r5 = mul2(gcg, wt), r6 = mul2(gcb, wt), r7 = mul2(dlda, a);
-          acc[4] = r4.x + r4.y;
-          acc[5] = r5.x + r5.y;
-          acc[6] = r6.x + r6.y;
-          acc[7] = r7.x + r7.y;
-        }
-        h = fma2(om, h, mul2(a, gcc));
-        bt = mul2(bt, om);
+        acc[4] = fmaf(gcr.y, wt.y, gcr.x * wt.x);
+        acc[5] = fmaf(gcg.y, wt.y, gcg.x * wt.x);
+        acc[6] = fmaf(gcb.y, wt.y, gcb.x * wt.x);
+        acc[7] = fmaf(dlda.y, a.y, dlda.x * a.x);
+        h = make_float2(fmaf(om.x, h.x, a.x * gcc.x), fmaf(om.y, h.y, a.y * gcc.y));
+        bt = make_float2(bt.x * om.x, bt.y * om.y);
         if (__any_sync(kFull, f0 || f1)) warp_add(acc, kidx, gacc + (size_t)id * 8);
       }
     }
