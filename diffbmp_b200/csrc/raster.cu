@@ -322,6 +322,7 @@ struct TileWalker {
   static constexpr int NT = L::NT;
   static constexpr int NW = L::NW;
   static constexpr bool kGrid = KIND != ATLAS_F32;   // packed atlases carry a clearance grid
+  static constexpr bool kQuad = KIND == ATLAS_F32_QUAD || KIND == ATLAS_F16_QUAD || KIND == ATLAS_BF16_QUAD;
   // Pixel-pair walk (2 pixels per thread, fixed colours).  Its staged record
   // holds the opacity and colours as duplicated pairs:
   //   [0] (mx, my, hw, hh)  [1] A  [2] (op, op, r, r)  [3] (g, g, b, b)  [4] (toff, goff, gext, -)
@@ -618,9 +619,18 @@ struct TileWalker {
                      col_b = make_float2(c1.z, c1.w);
         const float2 gcc = make_float2(fmaf(gcr.x, col_r.x, fmaf(gcg.x, col_g.x, gcb.x * col_b.x)),
                                        fmaf(gcr.y, col_r.y, fmaf(gcg.y, col_g.y, gcb.y * col_b.y)));
-        const float2 dlda = mul2(tk, fma2(ga, bt, sub2(g, gcc, h)));
-        const float2 u = mul2(dlda, make_float2(f0 ? gx.x : 0.f, f1 ? gx.y : 0.f));
-        const float2 v = mul2(dlda, make_float2(f0 ? gy.x : 0.f, f1 ? gy.y : 0.f));
+        // dL/da and the mask-gradient terms: scalar for the quad layouts, packed
+        // for the others (each measured faster on B200)
+        float2 dlda, u, v;
+        if (kQuad) {
+          dlda = make_float2(tk.x * fmaf(ga.x, bt.x, gcc.x - h.x), tk.y * fmaf(ga.y, bt.y, gcc.y - h.y));
+          u = make_float2(dlda.x * (f0 ? gx.x : 0.f), dlda.y * (f1 ? gx.y : 0.f));
+          v = make_float2(dlda.x * (f0 ? gy.x : 0.f), dlda.y * (f1 ? gy.y : 0.f));
+        } else {
+          dlda = mul2(tk, fma2(ga, bt, sub2(g, gcc, h)));
+          u = mul2(dlda, make_float2(f0 ? gx.x : 0.f, f1 ? gx.y : 0.f));
+          v = mul2(dlda, make_float2(f0 ? gy.x : 0.f, f1 ? gy.y : 0.f));
+        }
         const float2 ex = add2(tx, g.nhx), ey = add2(ty, g.nhy);
         const float2 wt = mul2(a, tk);
         float acc[8];
