@@ -44,18 +44,31 @@ class FitConfig:
     headroom: float = 1.3
 
 
+def _upload(a: np.ndarray, device) -> torch.Tensor:
+    """Host array to the device through pinned memory, asynchronously on the
+    current stream: a copy from pageable memory would first wait for every
+    kernel queued on that stream, which on a busy device (a serving loop
+    admitting jobs) blocks the host for the duration of other jobs' work."""
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(device, non_blocking=True)
+
+
 def _dev_f32(a, device, copy=True):
     if isinstance(a, torch.Tensor):
         t = a.detach().to(device=device, dtype=torch.float32).contiguous()
         return t.clone() if copy and t.data_ptr() == a.data_ptr() else t
-    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(device)
+    return _upload(np.asarray(a, np.float32), device)
 
 
 class ImageFitter:
     """One fit-an-image job resident on the device."""
 
     def __init__(self, means2D, radii, rotations, opacities, colors, sel, atlas: Atlas, target,
-                 background=None, config: FitConfig | None = None, device=None):
+                 background=None, config: FitConfig | None = None, device=None, list_capacity: int | None = None):
+        """list_capacity: tile-list entries to provision.  By default the
+        current lists are counted on the device (one host synchronisation);
+        a caller that knows an upper bound (list_capacity_bound) avoids it.
+        A bound that turns out short is still exact: an overflowed binning
+        skips its step, and sync() grows the lists and replays it."""
         self.cfg = cfg = config or FitConfig()
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         dev = self.device
@@ -64,8 +77,8 @@ class ImageFitter:
         self.rotations = _dev_f32(rotations, dev).view(-1)
         self.opacities = _dev_f32(opacities, dev).view(-1)
         self.colors = _dev_f32(colors, dev).view(-1, 3)
-        self.sel = (sel if isinstance(sel, torch.Tensor) else torch.from_numpy(np.asarray(sel))).to(
-            device=dev, dtype=torch.int32).contiguous()
+        self.sel = (sel.to(device=dev, dtype=torch.int32) if isinstance(sel, torch.Tensor)
+                    else _upload(np.asarray(sel, np.int32), dev)).contiguous()
         self.N = int(self.radii.numel())
         # read-only images: no private copy is needed
         self.target = _dev_f32(target, dev, copy=False)
@@ -99,7 +112,11 @@ class ImageFitter:
                                 float(self.W - 1), float(self.H - 1), 2.0, float(min(self.H, self.W) // 4), 1)
         self.steps_enqueued = 0
         self.graph = None
-        self._grow(self._count())
+        self._host_state = None   # pinned (step count, loss) staged by stage_result()
+        if list_capacity is None:
+            self._grow(self._count())
+        else:
+            self.rz._ensure(self.cv, int(list_capacity))
 
     # -- capacity ----------------------------------------------------------
     def _count(self) -> int:
@@ -201,6 +218,20 @@ class ImageFitter:
 
     def loss(self) -> float:
         return float(self.loss_dev.item())
+
+    def stage_result(self):
+        """Enqueues copies of the device step count and loss into pinned host
+        memory on the current stream; once that stream has passed them,
+        staged_result() reads them without synchronising."""
+        if self._host_state is None:
+            self._host_state = (torch.zeros(1, dtype=torch.int32).pin_memory(),
+                                torch.zeros(1, dtype=torch.float64).pin_memory())
+        self._host_state[0].copy_(self.step_count, non_blocking=True)
+        self._host_state[1].copy_(self.loss_dev, non_blocking=True)
+
+    def staged_result(self):
+        """(completed steps, loss) as staged by the last stage_result()."""
+        return int(self._host_state[0][0]), float(self._host_state[1][0])
 
     def render(self) -> torch.Tensor:
         """Current image (H,W,3) over the background (forward only)."""

@@ -56,17 +56,30 @@ class JobResult:
         return self.done - self.arrival
 
 
+def list_capacity_bound(spec, tile_size=32) -> int:
+    """Upper bound of a job's tile-list length from its parameters on the
+    host: the binning box of a primitive (its template's content box, rotated)
+    lies within the square of half-width r*sqrt(2) about its centre, and the
+    inclusive tile test adds at most one tile per side; non-finite geometry
+    is binned into every tile."""
+    H, W = spec.H, spec.W
+    tx, ty = (W + tile_size - 1) // tile_size, (H + tile_size - 1) // tile_size
+    r = np.abs(np.asarray(spec.radii, np.float64))
+    finite = np.isfinite(r) & np.isfinite(np.asarray(spec.rotations, np.float64)) & \
+        np.isfinite(np.asarray(spec.means2D, np.float64)).all(-1)
+    side = np.ceil(2.0 * np.sqrt(2.0) * np.where(finite, r, 0.0) / tile_size) + 2.0
+    per = np.minimum(side, tx) * np.minimum(side, ty)
+    return int(np.where(finite, per, tx * ty).sum()) + 4096
+
+
 def estimate_bytes(spec, tile_size=32) -> int:
     """Upper estimate of one job's resident device memory: target and
-    background images, per-pixel state, and tile lists sized as if every
-    primitive covered the tiles of its largest square (1.3x headroom, plus the
-    binning scratch of ~4 words per entry)."""
+    background images, per-pixel state, the tile lists at list_capacity_bound,
+    and the per-primitive state."""
     H, W, N = spec.H, spec.W, spec.N
     T = ((H + tile_size - 1) // tile_size) * ((W + tile_size - 1) // tile_size)
-    r = np.asarray(spec.radii, np.float64)
-    side = np.minimum(np.ceil(2.0 * r / tile_size) + 2.0, max(H, W) / tile_size + 1)
-    L = float(np.minimum(side * side, T).sum()) * 1.3 + 4096
-    return int(2 * H * W * 12 + H * W * 8 + L * 4 * 5 + N * 512 + (T + 1) * 4)
+    L = list_capacity_bound(spec, tile_size)
+    return int(2 * H * W * 12 + H * W * 8 + L * 4 + N * 512 + (T + 1) * 64)
 
 
 @dataclass
@@ -91,24 +104,44 @@ class Server:
         self.max_slots = max_slots
         self.budget = float(hbm_budget)
         self.streams = [torch.cuda.Stream() for _ in range(n_streams)]
+        self.admit_stream = torch.cuda.Stream()
         self.depth = depth
         self.graphs = graphs
         self.keep_params = keep_params
 
+    def _reserve(self, requests: List[JobRequest]):
+        """Grows the device allocator's cache to the jobs' estimated total
+        (within the HBM budget) before serving: job set-up then carves its
+        buffers from cached memory instead of allocating device memory while
+        the device is busy, which can stall the host for tens of milliseconds."""
+        want = min(self.budget, float(sum(estimate_bytes(r.spec, self.cfg.tile_size) for r in requests)))
+        free, _ = torch.cuda.mem_get_info()
+        want = int(min(want, 0.8 * free))
+        if want > (1 << 26):
+            block = torch.empty(want, dtype=torch.uint8, device="cuda")
+            del block
+
     def _admit(self, req: JobRequest, now: float, stream) -> _Slot:
+        """Sets a job up on the admission stream, which carries no iterations,
+        so its uploads never wait behind other jobs' work; the lists are sized
+        from list_capacity_bound (no device read-back).  The job's stream then
+        waits for the set-up."""
         s = req.spec
-        stream.wait_stream(torch.cuda.default_stream())   # job tensors may come from the default stream
-        with torch.cuda.stream(stream):
+        adm = self.admit_stream
+        adm.wait_stream(torch.cuda.default_stream())   # job tensors may come from the default stream
+        with torch.cuda.stream(adm):
             f = ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, self.atlas, s.target,
-                            s.background, self.cfg)
+                            s.background, self.cfg, list_capacity=list_capacity_bound(s, self.cfg.tile_size))
             if self.graphs:
                 f.capture()
+        stream.wait_stream(adm)
         return _Slot(req, f, stream, now)
 
     def run(self, requests: List[JobRequest], realtime=True) -> List[JobResult]:
         """Serves `requests`.  realtime: admit each at its arrival time (else
         all are queued at the start and latencies count from 0)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        self._reserve(requests)
         active: List[_Slot] = []
         results: List[JobResult] = []
         used = 0
@@ -116,9 +149,11 @@ class Server:
         clock = lambda: time.perf_counter() - t0
         load = {id(st): 0 for st in self.streams}        # active jobs per stream
         inflight = collections.deque()                   # events of issued iterations, in issue order
-        while pending or active:
+
+        def admit():
+            # arrived jobs, while slots and the HBM budget allow
+            nonlocal used
             now = clock()
-            # admission: arrived jobs, while slots and the HBM budget allow
             while pending and (pending[0].arrival <= now or not realtime) and len(active) < self.max_slots:
                 est = estimate_bytes(pending[0].spec, self.cfg.tile_size)
                 if used + est > self.budget and active:
@@ -131,6 +166,9 @@ class Server:
                 slot.nbytes = est
                 used += est
                 active.append(slot)
+
+        while pending or active:
+            admit()
             progressed = False
             for slot in list(active):
                 # retire finished iterations
@@ -139,10 +177,14 @@ class Server:
                     progressed = True
                 f = slot.fitter
                 if slot.issued >= slot.req.iterations and not slot.events:
+                    # the last iteration staged the step count and loss on the host;
+                    # only a skipped (overflowed) step needs the synchronising path
                     replayed = 0
-                    with torch.cuda.stream(slot.stream):
-                        replayed = f.sync()
-                        loss = f.loss()
+                    done, loss = f.staged_result()
+                    if done < f.steps_enqueued:
+                        with torch.cuda.stream(slot.stream):
+                            replayed = f.sync()
+                            loss = f.loss()
                     params = {k: v.detach().clone() for k, v in f.params().items()} if self.keep_params else None
                     # without realtime arrivals every request is queued at the start
                     arrival = slot.req.arrival if realtime else 0.0
@@ -152,11 +194,14 @@ class Server:
                     load[id(slot.stream)] -= 1
                     used -= slot.nbytes
                     progressed = True
+                    admit()   # the freed slot takes the next waiting job at once
                     continue
                 # issue up to `depth` iterations ahead of the host
                 while slot.issued < slot.req.iterations and len(slot.events) < self.depth:
                     with torch.cuda.stream(slot.stream):
                         f.step()
+                        if slot.issued + 1 == slot.req.iterations:
+                            f.stage_result()
                         ev = torch.cuda.Event()
                         ev.record(slot.stream)
                     slot.events.append(ev)
