@@ -54,3 +54,29 @@ def test_budget_limits_concurrency():
         assert b.admitted >= a.done - 1e-3
     s = serving.summarize(res)
     assert s["jobs"] == 6 and s["p99_s"] >= s["p50_s"] > 0
+
+
+def test_short_list_bound_replays_exactly(monkeypatch):
+    """A list-capacity bound that proves too short: every binning overflows
+    and skips its step on the device, retirement notices the missing steps
+    from the staged step count, grows the lists and replays them, and each
+    result still equals the job fitted alone."""
+    from diffbmp_b200 import serving
+    from diffbmp_b200.fitting import FitConfig, ImageFitter
+    from diffbmp_b200.rasterizer import Atlas
+    monkeypatch.setattr(serving, "list_capacity_bound", lambda spec, tile_size=32: 64)
+    atlas_np, reqs = _requests(4, 6, seed=5)
+    srv = serving.Server(torch.from_numpy(atlas_np).cuda(), kind="f16", fused=True, max_slots=4, n_streams=2)
+    res = {r.job_id: r for r in srv.run(reqs, realtime=False)}
+    assert sorted(res) == list(range(4))
+    assert all(r.replayed > 0 for r in res.values())
+    atlas = Atlas(torch.from_numpy(atlas_np).cuda(), "f16")
+    for req in reqs:
+        s = req.spec
+        f = ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, atlas, s.target, s.background,
+                        FitConfig(lr=0.01, fused=True))
+        for _ in range(req.iterations):
+            f.step()
+        f.sync()
+        r = res[req.job_id]
+        assert abs(f.loss() - r.loss) <= 1e-5 * abs(f.loss()) + 1e-9, (req.job_id, f.loss(), r.loss)
