@@ -389,19 +389,20 @@ def main():
 
     # --- e2e through the public API with host buffers ---------------------
     e2e_job = build_job(spec, HEADLINE_KIND, True, torch)
-    host = {k: torch.from_numpy(np.ascontiguousarray(getattr(spec, k), np.float32)).pin_memory()
-            for k in ("means2D", "radii", "rotations", "opacities", "colors")}
+    # the step's inputs: the five parameter arrays, packed host-side as
+    # ImageFitter.params_flat lays them out, uploaded with one copy
+    host = torch.from_numpy(np.concatenate([np.asarray(getattr(spec, k), np.float32).reshape(-1) for k in
+                                            ("means2D", "radii", "rotations", "opacities", "colors")])).pin_memory()
     loss_host = torch.zeros(2, dtype=torch.float64).pin_memory()   # ring of two step results
     done = [torch.cuda.Event(), torch.cuda.Event()]
-    dev_params = e2e_job.params()
-    h2d = sum(v.numel() * 4 for v in host.values())
+    dev_params = e2e_job.params_flat
+    h2d = host.numel() * 4
     losses = []
 
     def e2e_step(i):
         # one step in flight: step i is enqueued (inputs H2D, iteration, loss
         # D2H), then the host waits for step i - 1 and reads its loss
-        for k, v in host.items():
-            dev_params[k].copy_(v.view_as(dev_params[k]), non_blocking=True)
+        dev_params.copy_(host, non_blocking=True)
         e2e_job.step()
         loss_host[i % 2:i % 2 + 1].copy_(e2e_job.loss_dev, non_blocking=True)
         done[i % 2].record()

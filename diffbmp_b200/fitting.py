@@ -72,11 +72,20 @@ class ImageFitter:
         self.cfg = cfg = config or FitConfig()
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         dev = self.device
-        self.means2D = _dev_f32(means2D, dev).view(-1, 2)
-        self.radii = _dev_f32(radii, dev).view(-1)
-        self.rotations = _dev_f32(rotations, dev).view(-1)
-        self.opacities = _dev_f32(opacities, dev).view(-1)
-        self.colors = _dev_f32(colors, dev).view(-1, 3)
+        # the five parameter arrays are views of one (N*8,) buffer, params_flat
+        # (centres, radii, rotations, opacity logits, colour logits), so that a
+        # caller can upload all of them with one copy
+        parts = [_dev_f32(a, dev, copy=False).reshape(-1) for a in (means2D, radii, rotations, opacities, colors)]
+        n = int(parts[1].numel())
+        if [int(t.numel()) for t in parts] != [2 * n, n, n, n, 3 * n]:
+            raise ValueError("means2D (N,2), radii, rotations, opacities (N) and colors (N,3) disagree on N")
+        self.params_flat = torch.cat(parts) if n > 0 else torch.zeros(0, dtype=torch.float32, device=dev)
+        o = [0, 2 * n, 3 * n, 4 * n, 5 * n, 8 * n]
+        self.means2D = self.params_flat[o[0]:o[1]].view(-1, 2)
+        self.radii = self.params_flat[o[1]:o[2]]
+        self.rotations = self.params_flat[o[2]:o[3]]
+        self.opacities = self.params_flat[o[3]:o[4]]
+        self.colors = self.params_flat[o[4]:o[5]].view(-1, 3)
         self.sel = (sel.to(device=dev, dtype=torch.int32) if isinstance(sel, torch.Tensor)
                     else _upload(np.asarray(sel, np.int32), dev)).contiguous()
         self.N = int(self.radii.numel())
