@@ -512,9 +512,7 @@ struct TileWalker {
     const float2 m = pair_blend<false, false>(g, s, nullptr, nullptr);
     // a pixel may have stopped since the loads were issued
     const bool f0 = s.ok0 && f.live[0] && m.x > 1e-6f, f1 = s.ok1 && f.live[1] && m.y > 1e-6f;
-    float2 a = mul2(make_float2(c0.x, c0.y), m);
-    a.x = f0 ? a.x : 0.f;
-    a.y = f1 ? a.y : 0.f;
+    float2 a = make_float2(f0 ? c0.x * m.x : 0.f, f1 ? c0.y * m.y : 0.f);
     const float2 wt = make_float2(f.t.x * a.x, f.t.y * a.y);
     f.cr = make_float2(fmaf(wt.x, c0.z, f.cr.x), fmaf(wt.y, c0.w, f.cr.y));
     f.cg = make_float2(fmaf(wt.x, c1.x, f.cg.x), fmaf(wt.y, c1.y, f.cg.y));
@@ -607,9 +605,7 @@ struct TileWalker {
         const float2 m = pair_blend<true>(g, s, &gx, &gy);
         const float2 tx = s.tx, ty = s.ty;
         const bool f0 = s.ok0 && m.x > 1e-6f, f1 = s.ok1 && m.y > 1e-6f;
-        float2 a = mul2(make_float2(c0.x, c0.y), m);
-        a.x = f0 ? a.x : 0.f;
-        a.y = f1 ? a.y : 0.f;
+        float2 a = make_float2(f0 ? c0.x * m.x : 0.f, f1 ? c0.y * m.y : 0.f);
         const float2 om = make_float2(__saturatef(1.f - a.x), __saturatef(1.f - a.y));
         // T entering this fragment (see backward())
         const float2 tk = make_float2((pos == lp[0]) ? ts.x : __fdividef(ts.x, om.x),
