@@ -22,6 +22,7 @@ simple_tile_renderer.py:268-429) -- with a request loop:
 from __future__ import annotations
 
 import collections
+import gc
 import time
 from dataclasses import dataclass, field
 from typing import List, Optional
@@ -113,13 +114,20 @@ class Server:
         """Grows the device allocator's cache to the jobs' estimated total
         (within the HBM budget) before serving: job set-up then carves its
         buffers from cached memory instead of allocating device memory while
-        the device is busy, which can stall the host for tens of milliseconds."""
+        the device is busy, which stalled the host for up to 0.2 s.  The
+        allocator reuses a cached block only on the stream it was allocated
+        on, so the blocks are allocated on the admission stream: one large
+        block for the large pool, and 1 MB blocks for the small pool's
+        segments (tensors of up to 1 MB: counters, offsets, small jobs' state)."""
         want = min(self.budget, float(sum(estimate_bytes(r.spec, self.cfg.tile_size) for r in requests)))
         free, _ = torch.cuda.mem_get_info()
         want = int(min(want, 0.8 * free))
-        if want > (1 << 26):
-            block = torch.empty(want, dtype=torch.uint8, device="cuda")
-            del block
+        with torch.cuda.stream(self.admit_stream):
+            if want > (1 << 26):
+                block = torch.empty(want, dtype=torch.uint8, device="cuda")
+                del block
+            small = [torch.empty(1 << 20, dtype=torch.uint8, device="cuda") for _ in range(16 * len(requests))]
+            del small
 
     def _admit(self, req: JobRequest, now: float, stream) -> _Slot:
         """Sets a job up on the admission stream, which carries no iterations,
@@ -140,6 +148,18 @@ class Server:
     def run(self, requests: List[JobRequest], realtime=True) -> List[JobResult]:
         """Serves `requests`.  realtime: admit each at its arrival time (else
         all are queued at the start and latencies count from 0)."""
+        # the loop allocates an event per iteration: a garbage-collector pass in
+        # the middle of it would stall issuing, so collection pauses until the end
+        gc.collect()
+        gc_was_enabled = gc.isenabled()
+        gc.disable()
+        try:
+            return self._run(requests, realtime)
+        finally:
+            if gc_was_enabled:
+                gc.enable()
+
+    def _run(self, requests: List[JobRequest], realtime: bool) -> List[JobResult]:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         self._reserve(requests)
         active: List[_Slot] = []

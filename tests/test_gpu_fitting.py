@@ -89,3 +89,29 @@ def test_adam_matches_torch_optimizer(spec):
         ref["radii"].clamp_(2.0, float(min(spec.H, spec.W) // 4))
     for k, v in j.params().items():
         torch.testing.assert_close(v, ref[k].detach(), rtol=2e-5, atol=2e-5)
+
+
+def test_params_flat_layout_and_shape_check():
+    """The five parameter tensors are views of params_flat, in the order
+    centres, radii, rotations, opacity logits, colour logits; parameters that
+    disagree on N are rejected."""
+    import numpy as np
+    import pytest
+    import torch
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.fitting import FitConfig, ImageFitter
+    from diffbmp_b200.rasterizer import Atlas
+    s = wl.make_scene("c0", 1)
+    atlas = Atlas(torch.from_numpy(s.templates).cuda(), "f16q")
+    f = ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, atlas, s.target, s.background,
+                    FitConfig())
+    N = s.N
+    flat = f.params_flat.cpu().numpy()
+    want = np.concatenate([np.asarray(a, np.float32).reshape(-1)
+                           for a in (s.means2D, s.radii, s.rotations, s.opacities, s.colors)])
+    assert flat.shape == (8 * N,) and np.array_equal(flat, want)
+    for k, v in f.params().items():
+        assert v.untyped_storage().data_ptr() == f.params_flat.untyped_storage().data_ptr(), k
+    with pytest.raises(ValueError):
+        ImageFitter(s.means2D[:-1], s.radii, s.rotations, s.opacities, s.colors, s.sel, atlas, s.target,
+                    s.background, FitConfig())
