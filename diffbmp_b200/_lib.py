@@ -61,6 +61,8 @@ SIGNATURES = {
     "dbmp_psd_bboxes": (_i, [_vp, _vp, _i, _i, _i, _f, _vp, _vp, _vp]),
     "dbmp_psd_layout": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "dbmp_psd_layers": (_i, [_vp] * 6 + [_i, _i, _i] + [_vp] * 4 + [_i, _f, _f, _f, _vp, _vp, _vp]),
+    "dbmp_psd_rle_count": (_i, [_vp] * 4 + [_i, _ll, _i, _i] + [_vp] * 4),
+    "dbmp_psd_rle_write": (_i, [_vp] * 4 + [_i, _ll, _i, _i] + [_vp] * 4 + [_ll, _vp]),
     "dbmp_count": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_fused_fwd_bwd": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_adam_step": (_i, [_CP, ctypes.c_void_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

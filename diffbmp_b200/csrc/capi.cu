@@ -70,6 +70,10 @@ int launch_psd_layers(int N, int P, int Ht, int Wt, float scale, float alpha_max
                       const float* vis, const float* tmpl, const int* sel, const int* bbox,
                       const long long* layer_offsets, const long long* blk, const float* colors_orig, uint8_t* out,
                       cudaStream_t st);
+int launch_psd_rle(bool write, const uint8_t* layers, const int* sizes, const long long* layer_off,
+                   const long long* group_base, int N, long long G, unsigned order, int width_limit,
+                   unsigned short* row_bytes, int* group_tot, int* alpha_any, const long long* chan_off,
+                   const long long* group_dst, uint8_t* out, long long out_bytes, cudaStream_t st);
 
 // Validates a canvas description and derives the launch geometry.
 int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
@@ -366,6 +370,51 @@ int dbmp_psd_layers(const float* means2D, const float* radii, const float* rotat
   return launch_psd_layers(N, P, Ht, Wt, scale, alpha_max, c_blend, means2D, radii, rotations, colors, visibility,
                            templates, sel, bbox, (const long long*)layer_offsets, (const long long*)block_offsets,
                            colors_orig, out, (cudaStream_t)stream);
+}
+
+static int check_psd_rle(const char* who, const uint8_t* layers, const int32_t* sizes, const int64_t* layer_offsets,
+                         const int64_t* group_base, int N, long long num_groups, int channel_order,
+                         int width_limit, const uint16_t* row_bytes) {
+  REQUIRE(N >= 0 && num_groups >= 0, "%s: N=%d num_groups=%lld", who, N, num_groups);
+  REQUIRE(width_limit >= 1 && width_limit <= 30000, "%s: width_limit %d outside [1, 30000] (PSD limit)", who,
+          width_limit);
+  REQUIRE(((unsigned)channel_order & ~0x03030303u) == 0, "%s: channel_order 0x%08x: each byte must be 0..3", who,
+          (unsigned)channel_order);
+  if (N == 0 || num_groups == 0) return DBMP_OK;
+  REQUIRE(layers && sizes && layer_offsets && group_base && row_bytes, "%s: null pointer", who);
+  REQUIRE(((uintptr_t)layers & 3) == 0 && ((uintptr_t)sizes & 3) == 0 && ((uintptr_t)row_bytes & 7) == 0,
+          "%s: layers and sizes must be 4-byte and row_bytes 8-byte aligned", who);
+  return DBMP_OK;
+}
+
+int dbmp_psd_rle_count(const uint8_t* layers, const int32_t* sizes, const int64_t* layer_offsets,
+                       const int64_t* group_base, int N, long long num_groups, int channel_order, int width_limit,
+                       uint16_t* row_bytes, int32_t* group_totals, int32_t* alpha_any, void* stream) {
+  int rc = check_psd_rle("dbmp_psd_rle_count", layers, sizes, layer_offsets, group_base, N, num_groups,
+                         channel_order, width_limit, row_bytes);
+  if (rc != DBMP_OK) return rc;
+  if (N == 0 || num_groups == 0) return DBMP_OK;
+  REQUIRE(group_totals && ((uintptr_t)group_totals & 15) == 0,
+          "dbmp_psd_rle_count: group_totals must be non-null and 16-byte aligned");
+  return launch_psd_rle(false, layers, sizes, (const long long*)layer_offsets, (const long long*)group_base, N,
+                        num_groups, (unsigned)channel_order, width_limit, (unsigned short*)row_bytes, group_totals,
+                        alpha_any, nullptr, nullptr, nullptr, 0, (cudaStream_t)stream);
+}
+
+int dbmp_psd_rle_write(const uint8_t* layers, const int32_t* sizes, const int64_t* layer_offsets,
+                       const int64_t* group_base, int N, long long num_groups, int channel_order, int width_limit,
+                       const uint16_t* row_bytes, const int64_t* channel_offsets, const int64_t* group_offsets,
+                       uint8_t* out, long long out_bytes, void* stream) {
+  int rc = check_psd_rle("dbmp_psd_rle_write", layers, sizes, layer_offsets, group_base, N, num_groups,
+                         channel_order, width_limit, row_bytes);
+  if (rc != DBMP_OK) return rc;
+  REQUIRE(out_bytes >= 0, "dbmp_psd_rle_write: out_bytes %lld < 0", out_bytes);
+  if (N == 0 || num_groups == 0) return DBMP_OK;
+  REQUIRE(channel_offsets && group_offsets && (out || out_bytes == 0), "dbmp_psd_rle_write: null pointer");
+  return launch_psd_rle(true, layers, sizes, (const long long*)layer_offsets, (const long long*)group_base, N,
+                        num_groups, (unsigned)channel_order, width_limit, (unsigned short*)row_bytes, nullptr,
+                        nullptr, (const long long*)channel_offsets, (const long long*)group_offsets, out, out_bytes,
+                        (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -204,6 +204,241 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
   }
 }
 
+// ---------------------------------------------------------------------------
+// PSD file assembly: PackBits (RLE) channel data.
+//
+// The reference hands each cropped layer to psd-tools (PixelLayer.frompil,
+// then PSDImage.save; psd_export_uint8.py:153-186, psd_exporter.py:468-501),
+// which splits it into planes and RLE-compresses them row by row on the host.
+// Here every (layer, channel, row) is encoded on the device.  Rows are taken
+// 32 at a time, one warp per group of 32 rows of a layer and one lane per
+// row; each lane runs four encoders at once, one per RGBA byte, on uchar4
+// pixels that the warp stages through shared memory 32 rows x 32 pixels at a
+// time (coalesced loads, conflict-free reads with a 33-word row pitch).
+//
+// Encoding rule (a valid PackBits stream; a packet never crosses a row):
+//   - a maximal run of L >= 3 equal bytes becomes replicate packets
+//     [1-k, v] of k = min(remaining, 128) bytes each; a one-byte remainder
+//     becomes the literal packet [0, v];
+//   - maximal runs of one or two bytes are gathered into literal segments,
+//     written as packets [k-1, k bytes] of 128 bytes and a last shorter one.
+// The count pass writes each row's encoded size (at most w + ceil(w/128)
+// bytes, so 16 bits suffice for w <= 30000, the PSD width limit) and each
+// group's per-channel totals; the host plans where every channel block goes;
+// the write pass re-encodes and stores.  Each store is checked against the
+// planned extent of its row and the output size, so a plan that does not
+// match the data can write wrong bytes but never out of bounds.
+// ---------------------------------------------------------------------------
+
+constexpr int kRleWarps = 8;      // warps per CTA
+constexpr int kRlePitch = 33;     // words per staged row (32 pixels + 1 pad)
+constexpr int kRleMaxWidth = 30000;
+
+struct RleArgs {
+  const uint8_t* layers;        // packed RGBA crops, row-major per layer
+  const int* sizes;             // (N,2) w, h
+  const long long* layer_off;   // (N) byte offset of each crop
+  const long long* group_base;  // (N+1) exclusive prefix of ceil(h/32)
+  long long G;                  // number of row groups
+  int N;
+  unsigned order;               // byte index (0..3) of channel slot s in bits 8s..8s+1
+  int width_limit;
+  unsigned short* row_bytes;    // (G*32, 4) encoded size of each row's four channels
+  int* group_tot;               // (G, 4) per-group totals (count pass)
+  int* alpha_any;               // (N) 1 if a layer has a nonzero byte 3 (count pass; may be null)
+  const long long* chan_off;    // (N, 4) channel block offsets in out, < 0 skips (write pass)
+  const long long* group_dst;   // (G, 4) output offset of the group's first row (write pass)
+  uint8_t* out;                 // (write pass)
+  long long out_bytes;
+};
+
+// Four PackBits encoders of one row.  COUNT only adds sizes; WRITE stores.
+template <bool WRITE>
+struct RleRow {
+  int prev[4], run[4], lit[4], lst[4];
+  long long pos[4], lim[4];
+  const uint8_t* row;   // the row's first pixel (literal bytes are re-read from here)
+  unsigned order;
+  uint8_t* out;
+
+  __device__ __forceinline__ void put(int s, unsigned v) {
+    if (WRITE && pos[s] < lim[s]) out[pos[s]] = (uint8_t)v;
+    ++pos[s];
+  }
+  __device__ __forceinline__ void literal(int s, int start, int k) {
+    if (!WRITE) { pos[s] += 1 + k; return; }
+    put(s, (unsigned)(k - 1));
+    const int b = (order >> (8 * s)) & 3;
+    for (int j = 0; j < k; ++j) put(s, row[(long long)(start + j) * 4 + b]);
+  }
+  // Closes the run of run[s] bytes equal to prev[s] that ends before x = end.
+  __device__ __forceinline__ void close(int s, int end) {
+    const int L = run[s];
+    if (L >= 3) {
+      if (lit[s] > 0) literal(s, lst[s], lit[s]);
+      lit[s] = 0;
+      lst[s] = end;
+      if (!WRITE) { pos[s] += 2 * ((L + 127) >> 7); return; }
+      for (int rem = L; rem > 0; rem -= 128) {
+        const int k = min(rem, 128);
+        put(s, k >= 2 ? (unsigned)(1 - k) & 0xFFu : 0u);
+        put(s, (unsigned)prev[s]);
+      }
+    } else {
+      lit[s] += L;
+      if (lit[s] >= 128) {
+        literal(s, lst[s], 128);
+        lst[s] += 128;
+        lit[s] -= 128;
+      }
+    }
+  }
+  __device__ __forceinline__ void push(int s, int v, int x) {
+    if (v == prev[s]) { ++run[s]; return; }
+    close(s, x);
+    prev[s] = v;
+    run[s] = 1;
+  }
+  __device__ __forceinline__ void finish(int s, int w) {
+    close(s, w);
+    if (lit[s] > 0) literal(s, lst[s], lit[s]);
+  }
+};
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
+  __shared__ uint32_t stage[kRleWarps][32 * kRlePitch];
+  const int lane = threadIdx.x & 31;
+  uint32_t* sm = stage[threadIdx.x >> 5];
+  const long long nwarps = (long long)gridDim.x * kRleWarps;
+  for (long long g = (long long)blockIdx.x * kRleWarps + (threadIdx.x >> 5); g < a.G; g += nwarps) {
+    int lo = 0, hi = a.N;   // largest i with group_base[i] <= g
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (a.group_base[mid] <= g) lo = mid; else hi = mid;
+    }
+    const int i = lo;
+    const int w = a.sizes[2 * i], h = a.sizes[2 * i + 1];
+    const long long off = a.layer_off[i];
+    const bool ok = w >= 1 && w <= a.width_limit && h >= 1 && off >= 0 && (off & 3) == 0;
+    const long long y0 = (g - a.group_base[i]) * 32;
+    const int y = (int)y0 + lane;
+    const bool active = ok && y0 + lane < h;
+    const uint8_t* base = a.layers + (ok ? off : 0);
+
+    RleRow<WRITE> e;
+    e.order = a.order;
+    e.out = a.out;
+    e.row = base + (active ? (long long)y * w * 4 : 0);
+    unsigned short planned[4] = {0, 0, 0, 0};
+    bool skip = !ok;
+    if (WRITE) {
+      if (ok && active) {
+        const ushort4 rb = reinterpret_cast<const ushort4*>(a.row_bytes)[g * 32 + lane];
+        planned[0] = rb.x; planned[1] = rb.y; planned[2] = rb.z; planned[3] = rb.w;
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        int pre = planned[s];   // exclusive prefix over the group's rows
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, pre, d);
+          if (lane >= d) pre += t;
+        }
+        pre -= planned[s];
+        const long long co = ok ? a.chan_off[4 * i + s] : -1;
+        const long long gd = ok ? a.group_dst[4 * g + s] : -1;
+        if (co < 0 || gd < 0) {
+          e.pos[s] = 0; e.lim[s] = 0;   // every store of this slot is dropped
+        } else {
+          e.pos[s] = gd + pre;
+          e.lim[s] = min(e.pos[s] + planned[s], a.out_bytes);
+          if (active) {   // row byte count, big-endian, in the block's table; block header on row 0
+            const long long t = co + 2 + 2ll * y;
+            if (t + 1 < a.out_bytes) { a.out[t] = (uint8_t)(planned[s] >> 8); a.out[t + 1] = (uint8_t)planned[s]; }
+            if (y == 0 && co + 1 < a.out_bytes) { a.out[co] = 0; a.out[co + 1] = 1; }
+          }
+        }
+      }
+      skip = skip || (a.chan_off[4 * i] < 0 && a.chan_off[4 * i + 1] < 0 && a.chan_off[4 * i + 2] < 0 &&
+                      a.chan_off[4 * i + 3] < 0);
+    } else {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) { e.pos[s] = 0; e.lim[s] = 0; }
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) { e.prev[s] = -1; e.run[s] = 0; e.lit[s] = 0; e.lst[s] = 0; }
+
+    uint32_t any_alpha = 0;
+    if (!skip) {   // warp-uniform: skip depends on the layer only
+      for (int x0 = 0; x0 < w; x0 += 32) {
+        __syncwarp();
+#pragma unroll 4
+        for (int r = 0; r < 32; ++r) {
+          uint32_t v = 0;
+          if (y0 + r < h && x0 + lane < w)
+            v = *reinterpret_cast<const uint32_t*>(base + ((y0 + r) * (long long)w + x0 + lane) * 4);
+          sm[r * kRlePitch + lane] = v;
+        }
+        __syncwarp();
+        if (active) {
+          const int n = min(32, w - x0);
+          for (int x = 0; x < n; ++x) {
+            const uint32_t p = sm[lane * kRlePitch + x];
+            any_alpha |= p & 0xFF000000u;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) e.push(s, (p >> (8 * ((a.order >> (8 * s)) & 3))) & 0xFF, x0 + x);
+          }
+        }
+      }
+      if (active) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) e.finish(s, w);
+      }
+    }
+    if (!WRITE) {
+      int c[4];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) c[s] = active && !skip ? (int)e.pos[s] : 0;
+      reinterpret_cast<ushort4*>(a.row_bytes)[g * 32 + lane] =
+          make_ushort4((unsigned short)c[0], (unsigned short)c[1], (unsigned short)c[2], (unsigned short)c[3]);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) c[s] += __shfl_xor_sync(0xffffffffu, c[s], d);
+      }
+      if (lane == 0) reinterpret_cast<int4*>(a.group_tot)[g] = make_int4(c[0], c[1], c[2], c[3]);
+      if (__any_sync(0xffffffffu, any_alpha != 0) && lane == 0 && a.alpha_any) a.alpha_any[i] = 1;
+    }
+  }
+}
+
+int launch_psd_rle(bool write, const uint8_t* layers, const int* sizes, const long long* layer_off,
+                   const long long* group_base, int N, long long G, unsigned order, int width_limit,
+                   unsigned short* row_bytes, int* group_tot, int* alpha_any, const long long* chan_off,
+                   const long long* group_dst, uint8_t* out, long long out_bytes, cudaStream_t st) {
+  if (G == 0 || N == 0) return DBMP_OK;
+  const RleArgs a{layers, sizes, layer_off, group_base, G, N, order, width_limit, row_bytes, group_tot,
+                  alpha_any, chan_off, group_dst, out, out_bytes};
+  // Persistent grid: as many CTAs as are resident at once (148 SMs x the
+  // kernel's occupancy), so the grid-stride loop balances the row groups.
+  static int resident[2] = {0, 0};
+  if (resident[write] == 0) {
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (write) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<true>, kRleWarps * 32, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<false>, kRleWarps * 32, 0);
+    resident[write] = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 148);
+  }
+  long long ctas = (G + kRleWarps - 1) / kRleWarps;
+  if (ctas > resident[write]) ctas = resident[write];
+  if (write) psd_rle_kernel<true><<<(int)ctas, kRleWarps * 32, 0, st>>>(a);
+  else psd_rle_kernel<false><<<(int)ctas, kRleWarps * 32, 0, st>>>(a);
+  DBMP_CHECK_LAUNCH("psd_rle_kernel");
+  return DBMP_OK;
+}
+
 int launch_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale, int* bbox,
                       int* sizes, cudaStream_t st) {
   if (N == 0) return DBMP_OK;

@@ -304,6 +304,38 @@ int dbmp_psd_layers(const float* means2D, const float* radii, const float* rotat
                     const int64_t* block_offsets, int N, float scale, float alpha_max, float c_blend,
                     const float* colors_orig, uint8_t* out, void* stream);
 
+/* PSD file assembly, count pass: PackBits (RLE) sizes of every row of every
+ * channel of N packed uint8 RGBA images (layer n at byte layer_offsets[n],
+ * a multiple of 4, with (w,h) = sizes[n]; e.g. the output of dbmp_psd_layers).
+ * Rows are taken in groups of 32 per layer: group_base (N+1) i64 is the
+ * exclusive prefix sum of ceil(h/32) and num_groups = group_base[N].
+ * channel_order gives, in byte s, which RGBA byte (0..3) is channel slot s
+ * (0x02010003 = A,R,G,B as in layer records; 0x03020100 = R,G,B,A as in the
+ * merged image).  Writes row_bytes ((num_groups*32, 4) u16, 8-byte aligned:
+ * the encoded size of row 32*g+j of slot s at [(32*g + j)*4 + s], 0 past the
+ * layer's last row), group_totals ((num_groups, 4) i32, 16-byte aligned) and,
+ * if alpha_any is not null, alpha_any[n] = 1 for each layer with a nonzero
+ * byte 3 (the caller zeroes it first).  Images wider than width_limit
+ * (<= 30000, the PSD limit) are encoded as empty.  Replaces the per-layer
+ * psd-tools calls of cuda_tile_rasterizer/psd_export_uint8.py:153-186
+ * (PixelLayer.frompil, RLE compression at PSDImage.save,
+ * pydiffbmp/util/psd_exporter.py:494-501). */
+int dbmp_psd_rle_count(const uint8_t* layers, const int32_t* sizes, const int64_t* layer_offsets,
+                       const int64_t* group_base, int N, long long num_groups, int channel_order, int width_limit,
+                       uint16_t* row_bytes, int32_t* group_totals, int32_t* alpha_any, void* stream);
+
+/* PSD file assembly, write pass: for each image n with channel_offsets
+ * (N,4) i64 >= 0, writes slot s's PSD channel block at out +
+ * channel_offsets[4n+s]: the compression word 1 (RLE), the h big-endian u16
+ * row sizes and the rows' PackBits data, which starts for group g at
+ * group_offsets[4g+s] (i64, (num_groups, 4)).  The caller plans both from
+ * dbmp_psd_rle_count's outputs (block size = 2 + 2h + the slot's total).
+ * Every store is bounded by its row's planned size and by out_bytes. */
+int dbmp_psd_rle_write(const uint8_t* layers, const int32_t* sizes, const int64_t* layer_offsets,
+                       const int64_t* group_base, int N, long long num_groups, int channel_order, int width_limit,
+                       const uint16_t* row_bytes, const int64_t* channel_offsets, const int64_t* group_offsets,
+                       uint8_t* out, long long out_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
