@@ -206,6 +206,8 @@ def write_psd(f, width, height, records, layer_blob, merged_blocks):
         head = struct.pack(">h", -len(records)) + b"".join(records)
         size = len(head) + sum(len(memoryview(b)) for b in blobs)
         pad = size & 1
+        if 4 + size + pad + 4 > 0xFFFFFFFF:
+            raise ValueError(f"layer data of {size} bytes exceeds the 4 GiB a PSD (version 1) section can hold")
         f.write(struct.pack(">II", 4 + size + pad + 4, size + pad))
         f.write(head)
         for b in blobs:

@@ -119,6 +119,14 @@ def test_document_rejects_oversize_canvas():
         write_psd(io.BytesIO(), 30001, 10, [], [], [b"\0\1"] * 4)
 
 
+def test_document_rejects_layer_data_beyond_4gib():
+    from diffbmp_b200.psd import layer_record, write_psd
+    rec = layer_record(0, 0, 1, 1, [2, 2, 2, 2], "x")
+    huge = np.lib.stride_tricks.as_strided(np.zeros(1, np.uint8), (1 << 32,), (0,))   # 4 GiB, no memory
+    with pytest.raises(ValueError, match="4 GiB"):
+        write_psd(io.BytesIO(), 1, 1, [rec], [huge], [b"\0\1\0\2"] * 4)
+
+
 def test_layer_record_name_padding():
     from diffbmp_b200.psd import _pascal4
     for name in ("", "a", "abc", "abcd", "x" * 300):
