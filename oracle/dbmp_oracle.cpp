@@ -607,4 +607,53 @@ int orc_psd_layers(const float* means2D, const float* radii, const float* rot, c
   return 0;
 }
 
+// PackBits encoding of `rows` rows of `w` bytes: byte x of row y is
+// src[y * row_pitch + x * stride], so one channel of an interleaved RGBA image
+// is encoded in place.  Same rule as packbits_encode in oracle/psd_file.py
+// (runs of >= 3 equal bytes -> replicate packets of <= 128 bytes, a one-byte
+// remainder -> a one-byte literal; shorter runs gathered into literal packets
+// of <= 128 bytes).  Writes the encodings back to back into out and each
+// row's size into row_bytes; returns the total, or -1 if out_cap is too small.
+long long orc_packbits_rows(const uint8_t* src, int rows, int w, long long row_pitch, int stride, uint8_t* out,
+                            long long out_cap, int32_t* row_bytes) {
+  long long pos = 0;
+  auto put = [&](uint8_t v) { if (pos < out_cap) out[pos] = v; ++pos; };
+  for (int y = 0; y < rows; ++y) {
+    const uint8_t* r = src + (long long)y * row_pitch;
+    const long long start = pos;
+    int lit_start = 0, lit = 0;
+    auto flush = [&]() {
+      for (int k = 0; k < lit; k += 128) {
+        const int n = std::min(128, lit - k);
+        put((uint8_t)(n - 1));
+        for (int j = 0; j < n; ++j) put(r[(long long)(lit_start + k + j) * stride]);
+      }
+      lit = 0;
+    };
+    int x = 0;
+    while (x < w) {
+      const uint8_t v = r[(long long)x * stride];
+      int e = x + 1;
+      while (e < w && r[(long long)e * stride] == v) ++e;
+      const int L = e - x;
+      if (L >= 3) {
+        flush();
+        for (int rem = L; rem > 0; rem -= 128) {
+          const int k = std::min(rem, 128);
+          put(k >= 2 ? (uint8_t)(1 - k) : (uint8_t)0);
+          put(v);
+        }
+        lit_start = e;
+      } else {
+        if (lit == 0) lit_start = x;
+        lit += L;
+      }
+      x = e;
+    }
+    flush();
+    row_bytes[y] = (int32_t)(pos - start);
+  }
+  return pos <= out_cap ? pos : -1;
+}
+
 }  // extern "C"

@@ -14,8 +14,10 @@ a PackBits decoder.  The tests decode the device-written file with it and
 compare every layer plane, bound and name with the layer pixels, which are
 themselves bit-exact with the reference's CUDA kernel.
 
-``packbits_encode`` restates the library's own encoding rule so that the
-device's channel blocks can also be compared byte for byte:
+``packbits_encode`` (and ``packbits_rows_c``, the same rule compiled in
+dbmp_oracle.cpp, used as the timed CPU encoder) restates the library's own
+encoding rule so that the device's channel blocks can also be compared byte
+for byte:
   - a maximal run of L >= 3 equal bytes becomes replicate packets of
     min(remaining, 128) bytes ([1-k, v]); a one-byte remainder becomes the
     literal packet [0, v];
@@ -87,6 +89,26 @@ def packbits_decode(data, size: int) -> bytes:
     if len(out) != size:
         raise ValueError(f"row decodes to {len(out)} bytes, expected {size}")
     return bytes(out)
+
+
+def packbits_rows_c(plane: np.ndarray):
+    """The same encoding of every row of a (h, w) uint8 view (any strides) by
+    the compiled restatement in dbmp_oracle.cpp; returns (data, row sizes)."""
+    import ctypes
+    from oracle.oracle import lib
+    plane = np.asarray(plane)
+    h, w = plane.shape
+    if plane.dtype != np.uint8 or plane.strides[0] < 0 or plane.strides[1] < 1:
+        raise ValueError("a uint8 plane with positive strides is required")
+    out = np.empty(h * (w + (w + 127) // 128) + 1, np.uint8)
+    sizes = np.empty(max(h, 1), np.int32)
+    fn = lib().orc_packbits_rows
+    fn.restype = ctypes.c_longlong
+    n = fn(ctypes.c_void_p(plane.ctypes.data), h, w, ctypes.c_longlong(plane.strides[0]), plane.strides[1],
+           ctypes.c_void_p(out.ctypes.data), ctypes.c_longlong(out.size), ctypes.c_void_p(sizes.ctypes.data))
+    if n < 0:
+        raise RuntimeError("packbits output buffer too small")
+    return out[:n].tobytes(), sizes[:h]
 
 
 def channel_block(plane: np.ndarray) -> bytes:

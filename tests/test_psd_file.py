@@ -61,6 +61,20 @@ def test_packbits_round_trip_and_bound(i):
         pos += 2 + n if n < 128 else 2
 
 
+def test_compiled_packbits_matches_restatement():
+    rows = _rows()
+    rng = np.random.default_rng(9)
+    for row in rows[::3]:
+        a = np.frombuffer(row, np.uint8).reshape(1, -1)
+        data, sizes = O.packbits_rows_c(a)
+        assert data == O.packbits_encode(row) and sizes.tolist() == [len(data)]
+    img = (rng.integers(0, 3, (37, 301, 4)) * 70).astype(np.uint8)
+    for ch in range(4):                              # a strided channel of an interleaved image
+        data, sizes = O.packbits_rows_c(img[:, :, ch])
+        exp = [O.packbits_encode(img[y, :, ch].tobytes()) for y in range(37)]
+        assert data == b"".join(exp) and sizes.tolist() == [len(e) for e in exp]
+
+
 def test_packbits_decode_rejects_malformed():
     with pytest.raises(ValueError):
         O.packbits_decode(b"\x05\x01\x02", 6)       # literal runs past the data
