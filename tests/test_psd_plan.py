@@ -114,3 +114,60 @@ def test_planner_rejects_repeated_or_foreign_indices(planner):
             planner(*args, bad)
     with pytest.raises(ValueError):
         planner(*args[:4], 0x04000000, lambda a: np.arange(3))
+
+
+def test_exporter_order_names_and_filtering_on_cpu(monkeypatch, tmp_path):
+    """PSDExporter's host logic with the crops from the oracle's layer
+    restatement and the encoder stand-ins: background at the bottom, then the
+    kept primitives from the highest index up, named through the reference's
+    names[::-1][i] lookup; empty and transparent crops dropped."""
+    import diffbmp_b200.psd as P
+    from oracle import oracle as OO
+
+    def crops(templates, means2D, radii, rotations, vis_sig, colors_sig, sel, H, W, scale=1.0, alpha_max=1.0,
+              c_blend=0.0, colors_orig=None):
+        t = templates if templates.dim() == 3 else templates.unsqueeze(0)
+        m, r = means2D.numpy().astype(np.float32), radii.numpy().astype(np.float32)
+        bb, sz = OO.psd_bboxes(m, r, H, W, scale)
+        offs = np.concatenate([[0], np.cumsum(sz[:, 0].astype(np.int64) * sz[:, 1] * 4)[:-1]]).astype(np.int64)
+        buf, _ = OO.psd_layers(m, r, rotations.numpy().astype(np.float32), colors_sig.numpy().astype(np.float32),
+                               vis_sig.numpy().astype(np.float32), t.numpy().astype(np.float32),
+                               sel.numpy().astype(np.int32), bb, offs, scale, alpha_max)
+        return (torch.from_numpy(np.ascontiguousarray(buf, np.uint8)), torch.from_numpy(bb.astype(np.int32)),
+                torch.from_numpy(sz.astype(np.int32)), torch.from_numpy(offs))
+
+    for name, fn in (("call", _fake_call), ("_ptr", lambda t: t), ("_stream", lambda s=None: None),
+                     ("export_layers", crops)):
+        monkeypatch.setattr(P, name, fn)
+    rng = np.random.default_rng(0)
+    N, W, H = 25, 48, 40
+    f = lambda a: torch.from_numpy(np.asarray(a, np.float32))
+    tm = f(rng.uniform(0, 1, (3, 16, 16)))
+    x, y = f(rng.uniform(0, W, N)), f(rng.uniform(0, H, N))
+    r, th = f(rng.uniform(1, 8, N)), f(rng.uniform(-3, 3, N))
+    r[2], x[2], y[2] = 0.2, 10.5, 10.5                # a 1x1 crop: dropped
+    v, c = f(rng.normal(0, 2, N)), f(rng.normal(0, 2, (N, 3)))
+    v[5] = -60.0                                      # transparent
+    ex = P.PSDExporter(W, H, alpha_upper_bound=0.9, device="cpu")
+    ex.add_layers_batch_optimized(tm, x, y, r, th, v, c)
+    ex.add_background_layer((0.25, 0.5, 1.0))
+    doc = O.read_psd(open(ex.export_psd(str(tmp_path / "t.png")), "rb").read())
+
+    buf, bb, sz, offs = crops(tm, torch.stack([x, y], 1), r, th, torch.sigmoid(v), torch.sigmoid(c),
+                              ((N - 1 - torch.arange(N)) % 3).int(), H, W, 1.0, 0.9)
+    hb = buf.numpy()
+    kept = []
+    for i in range(N - 1, -1, -1):
+        w, h = (int(t) for t in sz[i])
+        a = hb[offs[i]:offs[i] + w * h * 4].reshape(h, w, 4)
+        if w > 1 and h > 1 and a[:, :, 3].max() > 0:
+            kept.append((i, a))
+    assert 5 not in [i for i, _ in kept] and 2 not in [i for i, _ in kept]
+    layers = doc["layers"]
+    assert layers[0]["name"] == "Background" and len(layers) == 1 + len(kept)
+    assert (O.layer_rgba(layers[0]) == np.array([63, 127, 255, 255], np.uint8)).all()
+    for got, (i, a) in zip(layers[1:], kept):
+        assert got["unicode_name"] == f"primitive_{N - 1 - i}"
+        assert (got["left"], got["top"], got["right"], got["bottom"]) == tuple(int(t) for t in bb[i])
+        np.testing.assert_array_equal(O.layer_rgba(got), a)
+    assert not doc["merged"].any()
