@@ -10,6 +10,11 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (runs the sm_100a kernels)")
+    # built libraries are not versioned: a fresh checkout compiles libdbmp.so
+    # (nvcc cross-compiles for sm_100a without a GPU) before any test loads it
+    if not os.path.exists(os.path.join(ROOT, "diffbmp_b200", "libdbmp.so")):
+        from diffbmp_b200 import build
+        build.build()
 
 
 def pytest_collection_modifyitems(config, items):
