@@ -104,58 +104,97 @@ def max_over_ranks(x, world):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons of the GPU, sampled during the timed
+    region by a host thread polling NVML about every millisecond (a timed
+    region of 20 steps lasts ~15 ms; nvidia-smi's 100 ms period would miss it),
+    with nvidia-smi as the fallback where NVML is unavailable."""
 
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index=0):
-        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
-        self.index = vis[index].strip() if index < len(vis) and vis[index].strip().isdigit() else str(index)
-        self.proc = None
-        self.lines = []
+    def __init__(self, index=0, period_s=0.001):
+        self.index, self.period = index, period_s
+        self.samples = []          # (sm_mhz, max_mhz, reason bitmask)
+        self.source = None
+        self._stop = threading.Event()
+        self._thread = self._proc = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:   # the CUDA device's own UUID (CUDA_VISIBLE_DEVICES may renumber devices)
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+            phys = int(vis[self.index]) if self.index < len(vis) and vis[self.index].strip().isdigit() else self.index
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(phys)
+
+    def _poll(self, nv, h):
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                break
+            time.sleep(self.period)
+
+    def _read_smi(self):
+        for line in self._proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            try:
+                mask = sum(bit for (name, bit), v in zip(self.REASONS.items(), f[5:9]) if v.lower() == "active")
+                self.samples.append((float(f[1]), float(f[2]), mask))
+            except (ValueError, IndexError):
+                continue
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            nv, h = self._nvml_handle()
+            self.source = "nvml, ~1 ms"
+            self._thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
         except Exception:
-            self.proc = None
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+            idx = vis[self.index].strip() if self.index < len(vis) and vis[self.index].strip().isdigit() \
+                else str(self.index)
+            try:
+                self._proc = subprocess.Popen(["nvidia-smi", f"--id={idx}", f"--query-gpu={self.QUERY}",
+                                               "--format=csv,noheader,nounits", "-lms", "100"],
+                                              stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi, 100 ms"
+                self._thread = threading.Thread(target=self._read_smi, daemon=True)
+            except Exception:
+                self._thread = None
+        if self._thread is not None:
+            self._thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
+        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                self.proc.wait(timeout=5)
+                self._proc.wait(timeout=5)
             except Exception:
-                self.proc.kill()
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
 
     def summary(self):
-        mhz, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                mhz.append(float(f[1])); mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not mhz:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(mhz)}
+        mhz = [s[0] for s in self.samples]
+        mask = 0
+        for s in self.samples:
+            mask |= int(s[2])
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": float(self.samples[-1][1]),
+                "reasons": sorted(n for n, bit in self.REASONS.items() if mask & bit),
+                "samples": len(self.samples), "source": self.source}
 
 
 def fp32_simt_peak_tflops(torch):
@@ -272,6 +311,69 @@ class CpuReference:
         return int(min(self.spec.H, max(base, seconds_per_sample / max(per_row, 1e-9))))
 
 
+PRECISION_KINDS = ("f32", "f16q", "f16", "bf16q", "bf16")
+
+
+def precision_band(spec, ts=32):
+    """Pixel rows [y0, y1) of the precision comparison: 8 tile rows at the
+    middle of the canvas (the whole canvas when it has at most 8 tile rows)."""
+    rows = 8 * ts
+    if spec.H <= rows:
+        return 0, spec.H
+    y0 = (spec.H // 2 - rows // 2) // ts * ts
+    return y0, y0 + rows
+
+
+def render_band(spec, kind, band, torch):
+    """Forward render of the scene (its initial parameters) with atlas storage
+    `kind`; returns the band's (color, alpha) on the host."""
+    from diffbmp_b200.rasterizer import Atlas, Rasterizer
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    atlas = Atlas(t(spec.templates), kind)
+    rz = Rasterizer(spec.H, spec.W, 32)      # the fit step's t_stop
+    color, alpha, _ = rz.forward(t(spec.means2D), t(spec.radii), t(spec.rotations), t(spec.opacities),
+                                 t(spec.colors), t(spec.sel), atlas)
+    y0, y1 = band
+    out = color[y0:y1].cpu().numpy(), alpha[y0:y1].cpu().numpy()
+    del color, alpha, atlas, rz
+    return out
+
+
+def precision_vs_oracle(spec, band, renders, ts=32):
+    """PSNR and max-abs error of each storage kind's image (rendered over the
+    scene's background) against the FP64 oracle's render of the same band of
+    rows (the reference kernels' semantics, every fragment, no termination)."""
+    from oracle import oracle as O
+    y0, y1 = band
+    tb = O.template_bboxes(spec.templates)
+    P, Ht, Wt = spec.templates.shape
+    offs, idx = O.bin_tiles(spec.H, spec.W, ts, spec.means2D, spec.radii, spec.rotations, spec.sel, tb, Ht, Wt)
+    tx = (spec.W + ts - 1) // ts
+    t0, t1 = (y0 // ts) * tx, ((y1 + ts - 1) // ts) * tx
+    so = (offs[t0:t1 + 1] - offs[t0]).astype(np.int32)
+    si = idx[offs[t0]:offs[t1]]
+    m = spec.means2D.astype(np.float64).copy()
+    m[:, 1] -= y0                  # exact in float64: the band's pixel offsets are unchanged
+    sc = O.Scene(y1 - y0, spec.W, ts, m, spec.radii, spec.rotations, spec.opacities, spec.colors, spec.templates,
+                 spec.sel, spec.alpha_max)
+    t_start = time.perf_counter()
+    ref = O.forward(sc, so, si)
+    t_oracle = time.perf_counter() - t_start
+    bg = spec.background[y0:y1].astype(np.float64)
+    ref_img = ref["color"] + (1.0 - ref["alpha"])[..., None] * bg
+    out = {"band": f"pixel rows {y0}-{y1 - 1} of {spec.H} ({(y1 - y0) // ts} tile rows), full width",
+           "checker": "FP64 oracle render (reference kernel semantics, every fragment, no termination)",
+           "image": "rendered = C + (1 - A) * background, PSNR with peak 1.0",
+           "oracle_s": t_oracle}
+    for kind, (color, alpha) in renders.items():
+        img = color.astype(np.float64) + (1.0 - alpha.astype(np.float64))[..., None] * bg
+        err = np.abs(img - ref_img)
+        mse = float(np.mean(err ** 2))
+        out[kind] = {"psnr_db": 10 * np.log10(1.0 / max(mse, 1e-30)), "max_abs": float(err.max()),
+                     "alpha_max_abs": float(np.abs(alpha - ref["alpha"]).max())}
+    return out
+
+
 def run_serving(n_jobs, seed, torch):
     """Serving workload: Poisson stream of fit-an-image jobs (canvas sides in
     {256,512,1024,2048}, N log-uniform in [256,20000], shared 16-bitmap atlas,
@@ -386,6 +488,17 @@ def main():
     pair = build_job(spec, "f16", True, torch)
     t_pair, _ = time_steps(pair, args.steps, args.warmup, torch, world)
     t_pair = max_over_ranks(t_pair, world)
+    t_bf16 = {}
+    for kind in ("bf16q", "bf16"):        # BF16 storage, quad and pair layouts
+        j = build_job(spec, kind, True, torch)
+        t, _ = time_steps(j, args.steps, args.warmup, torch, world)
+        t_bf16[kind] = max_over_ranks(t, world)
+        j.graph = None
+        del j
+    # precision renders: each storage kind's image of the scene's initial
+    # parameters, the band of rows compared with the FP64 oracle below
+    band = precision_band(spec)
+    renders = {kind: render_band(spec, kind, band, torch) for kind in PRECISION_KINDS}
 
     # --- e2e through the public API with host buffers ---------------------
     e2e_job = build_job(spec, HEADLINE_KIND, True, torch)
@@ -462,12 +575,18 @@ def main():
                        "what": "fused kernel, FP32 atlas in the reference layout"},
         "fused_f16_pair": {"iters_per_s": world * args.steps / t_pair, "ms_per_step": t_pair / args.steps * 1e3,
                            "what": "fused kernel, FP16 atlas as horizontal texel pairs (half the FP32 bytes)"},
+        "fused_bf16_quad": {"iters_per_s": world * args.steps / t_bf16["bf16q"],
+                            "ms_per_step": t_bf16["bf16q"] / args.steps * 1e3,
+                            "what": "fused kernel, BF16 bilinear-quad atlas"},
+        "fused_bf16_pair": {"iters_per_s": world * args.steps / t_bf16["bf16"],
+                            "ms_per_step": t_bf16["bf16"] / args.steps * 1e3,
+                            "what": "fused kernel, BF16 atlas as horizontal texel pairs"},
         "speedup_vs_plain_fp32": (world * args.steps / t_fused) / (world * args.steps / t_plain),
         "loss_after": loss_fused,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": FUSED_DRAM_BYTES,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                                       "kernel on this workload (profiles/fused_kernel_c2_f16quad.md)",
+                                       "kernel on this workload (the committed fused-kernel profile)",
                      "kernel": HEADLINE_KERNEL, "kernel_ms": t_kernel * 1e3,
                      "flop_model": "12*C + 144*F_live (C pairs passing cull, F_live fragments composited)",
                      "C": cand, "F_live": frag, "warp_entries": went, "live_pixel_slots": slots,
@@ -496,6 +615,9 @@ def main():
         ref = CpuReference(spec)
         rows = ref.rows_for_budget(15.0)          # about 15 s of CPU work
         t_cpu = ref.sample(rows)
+        # the same leg renders the precision band with the FP64 oracle, the
+        # checker of the storage kinds' images rendered above
+        line["precision"] = precision_vs_oracle(spec, band, renders)
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "iters/s", "cores": os.cpu_count(),
                                 "kind": "port",
                                 "sample": f"oracle fwd+bwd (reference algorithm, FP64, no termination) on {rows} of "

@@ -16,7 +16,7 @@ LIB_PATH = os.environ.get("DBMP_LIBRARY") or os.path.join(HERE, "libdbmp.so")
 
 DBMP_OK, DBMP_ERR_INVALID, DBMP_ERR_CUDA, DBMP_ERR_CAPACITY, DBMP_ERR_UNSUPPORTED = range(5)
 ATLAS_F32, ATLAS_F32_QUAD, ATLAS_F16_QUAD, ATLAS_BF16_QUAD, ATLAS_F16_PAIR, ATLAS_BF16_PAIR = range(6)
-BIN_CONTENT, BIN_CULL = 0, 1
+BIN_CONTENT, BIN_CULL, BIN_CONTENT_REF = 0, 1, 2
 
 # Every symbol include/dbmp.h declares, with (restype, argtypes).
 _vp, _i, _ll, _sz, _f = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_size_t, ctypes.c_float
@@ -65,6 +65,7 @@ SIGNATURES = {
     "dbmp_psd_rle_write": (_i, [_vp] * 4 + [_i, _ll, _i, _i] + [_vp] * 4 + [_ll, _vp]),
     "dbmp_count": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_fused_fwd_bwd": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_grads_from_accum": (_i, [_CP] + [_vp] * 11),
     "dbmp_adam_step": (_i, [_CP, ctypes.c_void_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 

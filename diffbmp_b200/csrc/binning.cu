@@ -193,9 +193,11 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
 
   if (rects == nullptr) return;
   int2 sx, sy;
-  if (bin_mode == DBMP_BIN_CONTENT) {
-    // vector_renderer.py:221-250 with the template of this primitive
-    const int q = valid ? tid : 0;
+  if (bin_mode == DBMP_BIN_CONTENT || bin_mode == DBMP_BIN_CONTENT_REF) {
+    // vector_renderer.py:221-250 with the bbox of this primitive's template,
+    // or, in the reference-exact mode, of template (N-1-n) % P as the
+    // reference always takes it (vector_renderer.py:220-226)
+    const int q = (bin_mode == DBMP_BIN_CONTENT_REF) ? (g.N - 1 - n) % g.P : (valid ? tid : 0);
     const float c32 = cosf(th), s32 = sinf(th);
     const float cu[4] = {tbbox[4 * q + 0], tbbox[4 * q + 1], tbbox[4 * q + 0], tbbox[4 * q + 1]};
     const float cv[4] = {tbbox[4 * q + 2], tbbox[4 * q + 2], tbbox[4 * q + 3], tbbox[4 * q + 3]};

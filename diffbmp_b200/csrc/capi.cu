@@ -193,10 +193,11 @@ int dbmp_bin(const dbmp_canvas* cv, const float* means2D, const float* radii, co
   Geom g;
   int rc = make_geom(cv, &g, "dbmp_bin");
   if (rc) return rc;
-  REQUIRE(cv->bin_mode == DBMP_BIN_CONTENT || cv->bin_mode == DBMP_BIN_CULL, "dbmp_bin: bin_mode %d unknown", cv->bin_mode);
+  REQUIRE(cv->bin_mode == DBMP_BIN_CONTENT || cv->bin_mode == DBMP_BIN_CULL || cv->bin_mode == DBMP_BIN_CONTENT_REF,
+          "dbmp_bin: bin_mode %d unknown", cv->bin_mode);
   REQUIRE(g.N == 0 || (means2D && radii && rotations && opacities && colors && sel && prim_info),
           "dbmp_bin: null pointer");
-  REQUIRE(cv->bin_mode != DBMP_BIN_CONTENT || tmpl_bbox, "dbmp_bin: tmpl_bbox is required in DBMP_BIN_CONTENT mode");
+  REQUIRE(cv->bin_mode == DBMP_BIN_CULL || tmpl_bbox, "dbmp_bin: tmpl_bbox is required in the DBMP_BIN_CONTENT modes");
   REQUIRE(tile_offsets && total_out && workspace, "dbmp_bin: null output or workspace");
   REQUIRE(capacity >= 0 && capacity <= 0x7fffffffll, "dbmp_bin: capacity %lld outside [0, 2^31)", capacity);
   REQUIRE(capacity == 0 || tile_indices, "dbmp_bin: tile_indices is null");
@@ -242,6 +243,20 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
   if (rc) return rc;
   return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
                          grad_rotations, grad_opacities, grad_colors, st);
+}
+
+int dbmp_grads_from_accum(const dbmp_canvas* cv, const double* grad_accum, const float* radii,
+                          const float* rotations, const float* opacities, const float* colors, float* grad_means2D,
+                          float* grad_radii, float* grad_rotations, float* grad_opacities, float* grad_colors,
+                          void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_grads_from_accum");
+  if (rc) return rc;
+  REQUIRE(g.N == 0 || (grad_accum && radii && rotations && opacities && colors), "dbmp_grads_from_accum: null input");
+  REQUIRE(g.N == 0 || (grad_means2D && grad_radii && grad_rotations && grad_opacities && grad_colors),
+          "dbmp_grads_from_accum: null output");
+  return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
+                         grad_rotations, grad_opacities, grad_colors, (cudaStream_t)stream);
 }
 
 int dbmp_forward_blend(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,

@@ -10,11 +10,14 @@
 //
 // The array holds kNoAllocMaxPrims primitives (4 MiB of device memory on
 // every GPU that loads the library, held until the process exits).  Its device
-// address is looked up once per device, on the first call made with that
-// device current; make that first call before any stream capture.  Every call
-// shares the one array and zeroes it before use: calls that overlap on the GPU
-// (on different streams, or from different host threads) race and must be
-// serialised by the caller.
+// address is looked up on the first call made with a device current, and again
+// whenever that device's context has changed since (a cudaDeviceReset reloads
+// the module, which can move the array); make the first call on each device
+// before any stream capture.  Every call shares the one array and zeroes it
+// before use: calls that overlap on the GPU (on different streams, or from
+// different host threads) race and must be serialised by the caller.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "dbmp_internal.cuh"
@@ -33,12 +36,42 @@ int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* 
 int launch_finalize(const Geom& g, const float* radii, const float* rot, const float* opac, const float* colors,
                     const double* gacc, float* gm, float* gr, float* grot, float* go, float* gc, cudaStream_t st);
 
+// Unique id of the calling thread's current CUDA context (0 if none or if the
+// driver does not provide it).  The driver entry points are taken through the
+// runtime, so the library needs no link-time dependency on the driver library.
+static unsigned long long current_context_id() {
+  using GetCurrentFn = CUresult (*)(CUcontext*);
+  using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(p);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx != nullptr &&
+      get_id(ctx, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
+
 // Device address of g_noalloc_accum on the current device (host code must not
 // use the symbol itself: on the host it is only a stand-in, not a device
-// address).
+// address).  Cached per device together with the id of the context it was
+// looked up in; a different context (or an unknown one) looks it up again.
 static int noalloc_scratch(double** out) {
   static std::mutex mu;
   static double* addr[kMaxDevices] = {};
+  static unsigned long long ctx_of[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_status(e, "dbmp_backward_noalloc: cudaGetDevice");
@@ -47,11 +80,13 @@ static int noalloc_scratch(double** out) {
     return DBMP_ERR_UNSUPPORTED;
   }
   std::lock_guard<std::mutex> lock(mu);
-  if (addr[dev] == nullptr) {
+  const unsigned long long ctx = current_context_id();
+  if (addr[dev] == nullptr || ctx == 0 || ctx != ctx_of[dev]) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_accum);
+    e = cudaGetSymbolAddress(&p, g_noalloc_accum);   // also makes the device's context current
     if (e != cudaSuccess) return cuda_status(e, "dbmp_backward_noalloc: cudaGetSymbolAddress");
     addr[dev] = static_cast<double*>(p);
+    ctx_of[dev] = current_context_id();
   }
   *out = addr[dev];
   return DBMP_OK;

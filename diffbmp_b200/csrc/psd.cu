@@ -14,6 +14,8 @@
 // psd_export_kernels.cu:26-55,96-195).
 #include <cstdint>
 
+#include <mutex>
+
 #include "dbmp_internal.cuh"
 
 namespace dbmp {
@@ -424,6 +426,26 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
   }
 }
 
+// CTAs of psd_rle_kernel<write> resident at once on the current device,
+// computed once per (device, pass) under a lock (devices may differ).
+static int rle_resident_ctas(bool write) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static int resident[kMaxDevices][2] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
+  std::lock_guard<std::mutex> lock(mu);
+  int& r = resident[dev][write ? 1 : 0];
+  if (r == 0) {
+    int per_sm = 0, sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (write) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<true>, kRleWarps * 32, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<false>, kRleWarps * 32, 0);
+    r = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 148);
+  }
+  return r;
+}
+
 int launch_psd_rle(bool write, const uint8_t* layers, const int* sizes, const long long* layer_off,
                    const long long* group_base, int N, long long G, unsigned order, int width_limit,
                    unsigned short* row_bytes, int* group_tot, int* alpha_any, const long long* chan_off,
@@ -431,19 +453,11 @@ int launch_psd_rle(bool write, const uint8_t* layers, const int* sizes, const lo
   if (G == 0 || N == 0) return DBMP_OK;
   const RleArgs a{layers, sizes, layer_off, group_base, G, N, order, width_limit, row_bytes, group_tot,
                   alpha_any, chan_off, group_dst, out, out_bytes};
-  // Persistent grid: as many CTAs as are resident at once (148 SMs x the
-  // kernel's occupancy), so the grid-stride loop balances the row groups.
-  static int resident[2] = {0, 0};
-  if (resident[write] == 0) {
-    int per_sm = 0, dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (write) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<true>, kRleWarps * 32, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<false>, kRleWarps * 32, 0);
-    resident[write] = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 148);
-  }
+  // Persistent grid: as many CTAs as are resident at once (the device's SMs x
+  // the kernel's occupancy), so the grid-stride loop balances the row groups.
+  const int resident = rle_resident_ctas(write);
   long long ctas = (G + kRleWarps - 1) / kRleWarps;
-  if (ctas > resident[write]) ctas = resident[write];
+  if (ctas > resident) ctas = resident;
   if (write) psd_rle_kernel<true><<<(int)ctas, kRleWarps * 32, 0, st>>>(a);
   else psd_rle_kernel<false><<<(int)ctas, kRleWarps * 32, 0, st>>>(a);
   DBMP_CHECK_LAUNCH("psd_rle_kernel");

@@ -23,7 +23,7 @@ import torch
 
 from . import _lib
 from ._lib import (ATLAS_BF16_PAIR, ATLAS_BF16_QUAD, ATLAS_F16_PAIR, ATLAS_F16_QUAD, ATLAS_F32, ATLAS_F32_QUAD,
-                   BIN_CONTENT, BIN_CULL, Canvas, DbmpError, call, lib)
+                   BIN_CONTENT, BIN_CONTENT_REF, BIN_CULL, Canvas, DbmpError, call, lib)
 
 # Atlas storage kinds: "f32" is the reference layout; the precision form
 # stores half / bfloat16 texels as horizontal pairs ("f16", "bf16", two 4-byte

@@ -50,6 +50,15 @@ typedef enum {
 #define DBMP_BIN_CULL 1     /* square cull box: the tight equivalent of the
                                all-primitives default mapping of
                                cuda_tile_rasterizer/tile_rasterize.cu:171-194 */
+#define DBMP_BIN_CONTENT_REF 2  /* as DBMP_BIN_CONTENT, but the content bbox of
+                               primitive i is always that of template
+                               (N-1-i) % P, whatever sel says, as the
+                               reference's binning takes it
+                               (vector_renderer.py:220-226).  Identical to
+                               DBMP_BIN_CONTENT when sel is that default; with
+                               another sel it reproduces the reference's lists,
+                               which can miss tiles of a primitive whose
+                               rendered template reaches beyond the bbox one. */
 
 typedef struct {
   int32_t height, width;      /* canvas in pixels */
@@ -127,11 +136,13 @@ int dbmp_prepare(const dbmp_canvas* cv, const float* means2D, const float* radii
  * = L).  When L > capacity the lists are not written, *total_out still holds
  * L and *overflow_out (device int32, may be null) is set to 1; call again with
  * capacity >= L.  capacity == 0 only counts.  tmpl_bbox is the output of
- * dbmp_template_bboxes (only read in DBMP_BIN_CONTENT mode).
+ * dbmp_template_bboxes (only read in the DBMP_BIN_CONTENT* modes).
  * Replaces VectorRenderer._unified_primitive_assignment
  * (pydiffbmp/core/renderer/vector_renderer.py:401-444) followed by
  * SimpleTileRenderer._convert_masks_to_mapping (simple_tile_renderer.py:721-766);
- * tile lists are bit-identical to the reference's in DBMP_BIN_CONTENT mode. */
+ * tile lists are bit-identical to the reference's in DBMP_BIN_CONTENT_REF
+ * mode for any sel, and in DBMP_BIN_CONTENT mode for sel = (N-1-i) % P (the
+ * renderer API's assignment, simple_tile_renderer.py:221-224). */
 int dbmp_bin(const dbmp_canvas* cv, const float* means2D, const float* radii,
              const float* rotations, const float* opacities, const float* colors,
              const int32_t* sel, const float* tmpl_bbox, void* prim_info,
@@ -180,8 +191,9 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
  * Limit: N <= dbmp_backward_noalloc_max_prims() (65536); larger N returns
  * DBMP_ERR_CAPACITY.  The array takes 4 MiB on every GPU that loads the
  * library, until exit.  The first call on a device looks up the array's
- * device address with that device current: make it before any stream
- * capture.  All calls share the array (zeroed by each call), so calls that
+ * device address with that device current, and a call after that device's
+ * context changed (cudaDeviceReset) looks it up again: make the first call
+ * on each device, and the first after a reset, before any stream capture.  All calls share the array (zeroed by each call), so calls that
  * overlap on the GPU race; serialise them.  No counterpart in the reference. */
 int dbmp_backward_noalloc(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
                           const int32_t* tile_offsets, const int32_t* tile_indices,
@@ -253,6 +265,18 @@ int dbmp_fused_fwd_bwd(const dbmp_canvas* cv, const void* prim_info, const void*
                        const float* target, const float* background, float* out_image,
                        double* grad_accum, double* loss_out, const int32_t* skip_flag,
                        void* stream);
+
+/* The reference's five gradient outputs from the raw per-primitive sums in
+ * grad_accum ((N,8) f64, as left by dbmp_fused_fwd_bwd), for callers that
+ * run their own optimiser after the fused step: grad_means2D (N,2),
+ * grad_radii, grad_rotations, grad_opacities (N), grad_colors (N,3), f32,
+ * overwritten, with the chain rule of dbmp_backward (the gradient-output
+ * stage of TileRasterizer::backward, cuda_tile_rasterizer/tile_rasterize.cu:
+ * 638-780, and tile_backward.cu:255-343). */
+int dbmp_grads_from_accum(const dbmp_canvas* cv, const double* grad_accum, const float* radii,
+                          const float* rotations, const float* opacities, const float* colors,
+                          float* grad_means2D, float* grad_radii, float* grad_rotations,
+                          float* grad_opacities, float* grad_colors, void* stream);
 
 /* Optimiser settings of dbmp_adam_step: learning rate per parameter in the
  * order x, y, r, theta, opacity, colour r/g/b; Adam betas/eps; clamp bounds. */

@@ -308,7 +308,8 @@ int orc_world_bboxes(const float* means2D, const float* radii, const float* rot,
   return 0;
 }
 
-// Tile lists.  mode 0: vector_renderer.py:401-444 _unified_primitive_assignment
+// Tile lists.  mode 0 (and 2, with the reference's bbox template choice):
+// vector_renderer.py:401-444 _unified_primitive_assignment
 // (world-bbox vs tile bounds, inclusive, float32 compare) followed by
 // simple_tile_renderer.py:721-766 _convert_masks_to_mapping (tiles row-major,
 // ascending primitive id).  mode 1: a tile holds a primitive iff some pixel of
@@ -322,13 +323,18 @@ long long orc_bin(int H, int W, int ts, const float* means2D, const float* radii
   const int tX = (W + ts - 1) / ts, tY = (H + ts - 1) / ts, T = tX * tY;
   std::vector<float> wb((size_t)N * 4);
   std::vector<int> bsel(sel, sel + N);
-  if (mode == 0) {
-    for (int n = 0; n < N; ++n) if (bsel[n] < 0 || bsel[n] >= P) bsel[n] = 0;
+  if (mode != 1) {
+    // mode 2: the bbox template of primitive n is (N-1-n) % P whatever sel
+    // says, as vector_renderer.py:220-226 takes it
+    for (int n = 0; n < N; ++n) {
+      if (mode == 2) bsel[n] = (N - 1 - n) % P;
+      else if (bsel[n] < 0 || bsel[n] >= P) bsel[n] = 0;
+    }
     orc_world_bboxes(means2D, radii, rot, bsel.data(), tbbox, N, P, wb.data());
   }
   // per-primitive tile-column / tile-row predicate
   auto colhit = [&](int n, int tx) -> bool {
-    if (mode == 0) {
+    if (mode != 1) {
       const float xs = (float)(tx * ts), xe = (float)std::min(tx * ts + ts, W);
       return !((wb[4 * n + 1] < xs) || (wb[4 * n + 0] > xe));
     }
@@ -343,7 +349,7 @@ long long orc_bin(int H, int W, int ts, const float* means2D, const float* radii
     return false;
   };
   auto rowhit = [&](int n, int ty) -> bool {
-    if (mode == 0) {
+    if (mode != 1) {
       const float ys = (float)(ty * ts), ye = (float)std::min(ty * ts + ts, H);
       return !((wb[4 * n + 3] < ys) || (wb[4 * n + 2] > ye));
     }

@@ -31,6 +31,7 @@ SEM_TORCH = 1    # the reference PyTorch per-tile path (grid_sample zeros paddin
 
 BIN_CONTENT = 0  # world bbox of the template's nonzero texels (renderer API)
 BIN_CULL = 1     # square cull box (equivalent to the all-primitives default mapping)
+BIN_CONTENT_REF = 2  # as BIN_CONTENT with the bbox of template (N-1-i) % P whatever sel says
 
 _lib = None
 
@@ -228,3 +229,43 @@ def boundary_band(scene: Scene, offs, idx, edge=1e-3, t_stop=0.0, nthreads=0):
     hi = forward(scene, offs, idx, SEM_KERNEL, t_stop, nthreads, edge=+edge)
     lo = forward(scene, offs, idx, SEM_KERNEL, t_stop, nthreads, edge=-edge)
     return np.abs(hi["color"] - lo["color"]).max(-1), np.abs(hi["alpha"] - lo["alpha"])
+
+
+def check_image(scene: Scene, offs, idx, color, alpha, tol=1e-5, ref=None, nthreads=0):
+    """Compares a float32 render (color (H,W,3), alpha (H,W)) with this
+    oracle's FP64 render.  Pixels outside the boundary band must be within
+    `tol` max-abs; pixels inside it (a fragment within 1e-3 px/texel of a
+    cull or texel-cut boundary, where any float rounding can flip it) within
+    the band's own spread + tol.  Raises AssertionError; returns a summary."""
+    ref = forward(scene, offs, idx, nthreads=nthreads) if ref is None else ref
+    band_c, band_a = boundary_band(scene, offs, idx, edge=1e-3, nthreads=nthreads)
+    ec = np.abs(np.asarray(color, np.float64) - ref["color"]).max(-1)
+    ea = np.abs(np.asarray(alpha, np.float64) - ref["alpha"])
+    sens = (band_c > 0) | (band_a > 0)
+    assert ec[~sens].max(initial=0) <= tol, ("color", ec[~sens].max(initial=0))
+    assert ea[~sens].max(initial=0) <= tol, ("alpha", ea[~sens].max(initial=0))
+    assert np.all(ec[sens] <= band_c[sens] + tol), ("color in band", float((ec - band_c)[sens].max()))
+    assert np.all(ea[sens] <= band_a[sens] + tol), ("alpha in band", float((ea - band_a)[sens].max()))
+    return dict(max_err=float(max(ec[~sens].max(initial=0), ea[~sens].max(initial=0))),
+                sensitive=int(sens.sum()), ref=ref)
+
+
+def check_grads(scene: Scene, offs, idx, grad_color, grad_alpha, ours, rel=1e-4, nthreads=0, verbose=True):
+    """Per parameter block k of the (N,8) gradients:
+    ||ours - oracle|| <= rel ||oracle|| + ||oracle(+edge) - oracle(-edge)||
+    (the band spread of the gradient, edge = 1e-3).  Returns the per-block
+    relative errors."""
+    ref = backward(scene, offs, idx, grad_color, grad_alpha, nthreads=nthreads)
+    hi = backward(scene, offs, idx, grad_color, grad_alpha, nthreads=nthreads, edge=1e-3)
+    lo = backward(scene, offs, idx, grad_color, grad_alpha, nthreads=nthreads, edge=-1e-3)
+    ours = np.asarray(ours, np.float64).reshape(scene.N, 8)
+    errs = []
+    for k in range(8):
+        spread = np.linalg.norm(hi[:, k] - lo[:, k])
+        err = np.linalg.norm(ours[:, k] - ref[:, k])
+        nrm = np.linalg.norm(ref[:, k])
+        if verbose:
+            print(f"  block {k}: err {err:.3e} |ref| {nrm:.3e} band {spread:.3e}")
+        assert err <= rel * nrm + spread + 1e-9, (k, err, nrm, spread)
+        errs.append(err / max(nrm, 1e-30))
+    return errs

@@ -29,7 +29,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("DIFFBMP_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("DIFFBMP_REFERENCE"),
+                    help="root of the reference checkout (or set DIFFBMP_REFERENCE)")
     ap.add_argument("--configs", default="c0")
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args()

@@ -57,6 +57,8 @@ class _StubFinder(importlib.abc.MetaPathFinder, importlib.abc.Loader):
 
 
 def load_reference(ref_root: str):
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "pydiffbmp")):
+        raise SystemExit(f"reference checkout not found at {ref_root!r}: pass --reference or set DIFFBMP_REFERENCE")
     os.environ["WANDB_MODE"] = "disabled"
     sys.meta_path.insert(0, _StubFinder())
     sys.path.insert(0, ref_root)
@@ -152,7 +154,8 @@ def gen_torch_case(str_, name, H, W, ts, S, N, seed, rmin, rmax, amax):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("DIFFBMP_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("DIFFBMP_REFERENCE"),
+                    help="root of the reference checkout (or set DIFFBMP_REFERENCE)")
     args = ap.parse_args()
     str_ = load_reference(args.reference)
     from diffbmp_b200 import workloads as wl
