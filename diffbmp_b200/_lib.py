@@ -26,7 +26,20 @@ class AdamCfg(ctypes.Structure):
     """Mirror of dbmp_adam_cfg."""
     _fields_ = [("lr", ctypes.c_float * 8), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
                 ("eps", ctypes.c_float), ("x_max", ctypes.c_float), ("y_max", ctypes.c_float),
-                ("r_min", ctypes.c_float), ("r_max", ctypes.c_float), ("clamp", ctypes.c_int32)]
+                ("r_min", ctypes.c_float), ("r_max", ctypes.c_float), ("clamp", ctypes.c_int32),
+                ("lr_gamma", ctypes.c_float)]
+
+
+class PruneCfg(ctypes.Structure):
+    """Mirror of dbmp_prune_cfg."""
+    _fields_ = [("every", ctypes.c_int32), ("num_iterations", ctypes.c_int32), ("no_prune_last", ctypes.c_int32),
+                ("warmup", ctypes.c_int32), ("threshold", ctypes.c_float), ("pool_rows", ctypes.c_int32)]
+
+
+class BlurSchedule(ctypes.Structure):
+    """Mirror of dbmp_blur_schedule."""
+    _fields_ = [("mode", ctypes.c_int32), ("sigma", ctypes.c_float), ("sigma_start", ctypes.c_float),
+                ("sigma_end", ctypes.c_float), ("num_iterations", ctypes.c_int32)]
 
 
 class Canvas(ctypes.Structure):
@@ -66,6 +79,8 @@ SIGNATURES = {
     "dbmp_count": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_fused_fwd_bwd": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_grads_from_accum": (_i, [_CP] + [_vp] * 11),
+    "dbmp_prune": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_template_blur_scheduled": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "dbmp_adam_step": (_i, [_CP, ctypes.c_void_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 

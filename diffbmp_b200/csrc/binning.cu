@@ -525,19 +525,18 @@ int launch_atlas_pack(const float* tmpl, int P, int Ht, int Wt, int kind, void* 
 // kernel, K = 2 round(3 sigma) + 1, weights k[i] k[j] of the normalised 1-D
 // Gaussian exp(-0.5 ((i - K/2) / sigma)^2), zero padding, same output size.
 // One thread per output texel; the 1-D weights sit in shared memory.
-__global__ void template_blur_kernel(const float* __restrict__ in, int P, int Ht, int Wt, int K, float sigma,
-                                     float* __restrict__ out) {
-  extern __shared__ float s_k[];
-  if (threadIdx.x == 0) {
-    float sum = 0.f;
-    for (int i = 0; i < K; ++i) {
-      const float a = (float)(i - K / 2) / sigma;
-      s_k[i] = expf(-0.5f * (a * a));
-      sum += s_k[i];
-    }
-    for (int i = 0; i < K; ++i) s_k[i] /= sum;
+__device__ __forceinline__ void blur_weights(float sigma, int K, float* s_k) {
+  float sum = 0.f;
+  for (int i = 0; i < K; ++i) {
+    const float a = (float)(i - K / 2) / sigma;
+    s_k[i] = expf(-0.5f * (a * a));
+    sum += s_k[i];
   }
-  __syncthreads();
+  for (int i = 0; i < K; ++i) s_k[i] /= sum;
+}
+
+__device__ __forceinline__ void blur_texels(const float* __restrict__ in, int P, int Ht, int Wt, int K,
+                                            const float* s_k, float* __restrict__ out) {
   const long long total = (long long)P * Ht * Wt;
   const int h = K / 2;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -557,6 +556,52 @@ __global__ void template_blur_kernel(const float* __restrict__ in, int P, int Ht
   }
 }
 
+__global__ void template_blur_kernel(const float* __restrict__ in, int P, int Ht, int Wt, int K, float sigma,
+                                     float* __restrict__ out) {
+  extern __shared__ float s_k[];
+  if (threadIdx.x == 0) blur_weights(sigma, K, s_k);
+  __syncthreads();
+  blur_texels(in, P, Ht, Wt, K, s_k, out);
+}
+
+// Kernel size of a blur sigma: 2 round(3 sigma) + 1 with Python's round (ties
+// to even, as rint does).
+__host__ __device__ inline int blur_kernel_size(double sigma) { return (int)(2.0 * rint(3.0 * sigma) + 1.0); }
+
+// The blur of one fit iteration it = *step_count under a schedule
+// (simple_tile_renderer.py:1015-1021): sigma in double as the reference's
+// Python computes it, the kernel size from that double, the weights in float
+// (gaussian_blur's float32 tensor arithmetic); sigma <= 0 copies.  The weight
+// buffer holds kmax entries, the largest kernel of the schedule.
+__global__ void template_blur_sched_kernel(const float* __restrict__ in, int P, int Ht, int Wt,
+                                           dbmp_blur_schedule sched, const int* __restrict__ step_count, int kmax,
+                                           float* __restrict__ out) {
+  extern __shared__ float s_k[];
+  __shared__ int s_K;
+  if (threadIdx.x == 0) {
+    double sigma = 0.0;
+    if (sched.mode == 1) {
+      sigma = (double)sched.sigma;
+    } else if (sched.mode == 2) {
+      const double progress = (double)*step_count / (double)sched.num_iterations;
+      sigma = (double)sched.sigma_start * (1.0 - progress) + (double)sched.sigma_end * progress;
+    }
+    int K = sigma > 0.0 ? blur_kernel_size(sigma) : 0;
+    if (K > kmax) K = kmax;      // cannot happen for a linear schedule between its two ends
+    if (K > 0) blur_weights((float)sigma, K, s_k);
+    s_K = K;
+  }
+  __syncthreads();
+  const int K = s_K;
+  if (K > 0) {
+    blur_texels(in, P, Ht, Wt, K, s_k, out);
+    return;
+  }
+  const long long total = (long long)P * Ht * Wt;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x)
+    out[t] = in[t];
+}
+
 int launch_template_blur(const float* in, int P, int Ht, int Wt, float sigma, float* out, cudaStream_t st) {
   const long long total = (long long)P * Ht * Wt;
   if (total == 0) return DBMP_OK;
@@ -565,12 +610,31 @@ int launch_template_blur(const float* in, int P, int Ht, int Wt, float sigma, fl
     cudaError_t e = cudaMemcpyAsync(out, in, sizeof(float) * (size_t)total, cudaMemcpyDeviceToDevice, st);
     return e == cudaSuccess ? DBMP_OK : cuda_status(e, "cudaMemcpyAsync(templates)");
   }
-  // K = 2 * round(3 sigma) + 1 with Python's round (ties to even), as rint does
-  const int K = (int)(2.0 * rint(3.0 * (double)sigma) + 1.0);
+  const int K = blur_kernel_size((double)sigma);
   if (K > 4097) { set_error("dbmp_template_blur: sigma %g gives a kernel of %d texels", (double)sigma, K); return DBMP_ERR_INVALID; }
   const int blocks = (int)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16);
   template_blur_kernel<<<blocks, 256, sizeof(float) * K, st>>>(in, P, Ht, Wt, K, sigma, out);
   DBMP_CHECK_LAUNCH("template_blur_kernel");
+  return DBMP_OK;
+}
+
+int launch_template_blur_sched(const float* in, int P, int Ht, int Wt, const dbmp_blur_schedule* sched,
+                               const int* step_count, float* out, cudaStream_t st) {
+  const long long total = (long long)P * Ht * Wt;
+  if (total == 0) return DBMP_OK;
+  // largest kernel over the schedule: sigma is constant or linear between its ends
+  double smax = 0.0;
+  if (sched->mode == 1) smax = sched->sigma;
+  if (sched->mode == 2) smax = sched->sigma_start > sched->sigma_end ? sched->sigma_start : sched->sigma_end;
+  const int kmax = smax > 0.0 ? blur_kernel_size(smax) : 1;
+  if (kmax > 4097) {
+    set_error("dbmp_template_blur_scheduled: sigma %g gives a kernel of %d texels", smax, kmax);
+    return DBMP_ERR_INVALID;
+  }
+  const int blocks = (int)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16);
+  template_blur_sched_kernel<<<blocks, 256, sizeof(float) * kmax, st>>>(in, P, Ht, Wt, *sched, step_count, kmax,
+                                                                         out);
+  DBMP_CHECK_LAUNCH("template_blur_sched_kernel");
   return DBMP_OK;
 }
 

@@ -51,12 +51,11 @@ int launch_finalize(const Geom& g, const float* radii, const float* rot, const f
 int launch_fused(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  const float* target, const float* background, float* out_image, double* gacc, double* loss,
                  const int* skip_flag, cudaStream_t st);
-struct AdamArgs {
-  float lr[8];
-  float beta1, beta2, eps;
-  float x_max, y_max, r_min, r_max;
-  int clamp;
-};
+int launch_prune(const Geom& g, const PruneArgs& a, const int* step_count, const float* pool, int* state,
+                 float* means2D, float* radii, float* rot, float* opac, float* colors, const int* skip_flag,
+                 cudaStream_t st);
+int launch_template_blur_sched(const float* in, int P, int Ht, int Wt, const dbmp_blur_schedule* sched,
+                               const int* step_count, float* out, cudaStream_t st);
 int launch_adam(const Geom& g, const AdamArgs& a, const double* gacc, float* means2D, float* radii, float* rot,
                 float* opac, float* colors, float* m1, float* m2, int* step_count, const int* skip_flag,
                 cudaStream_t st);
@@ -352,8 +351,35 @@ int dbmp_adam_step(const dbmp_canvas* cv, const dbmp_adam_cfg* cfg, const double
   a.beta1 = cfg->beta1; a.beta2 = cfg->beta2; a.eps = cfg->eps;
   a.x_max = cfg->x_max; a.y_max = cfg->y_max; a.r_min = cfg->r_min; a.r_max = cfg->r_max;
   a.clamp = cfg->clamp;
+  a.gamma = (cfg->lr_gamma == 0.f) ? 1.f : cfg->lr_gamma;
+  REQUIRE(a.gamma > 0.f && a.gamma <= 1e6f, "dbmp_adam_step: lr_gamma %g must be positive", (double)cfg->lr_gamma);
   return launch_adam(g, a, grad_accum, means2D, radii, rotations, opacities, colors, adam_m, adam_v, step_count,
                      skip_flag, (cudaStream_t)stream);
+}
+
+int dbmp_prune(const dbmp_canvas* cv, const dbmp_prune_cfg* cfg, const int32_t* step_count, const float* pool,
+               int32_t* state, float* means2D, float* radii, float* rotations, float* opacities, float* colors,
+               const int32_t* skip_flag, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_prune");
+  if (rc) return rc;
+  REQUIRE(cfg && step_count && state, "dbmp_prune: null cfg / step_count / state");
+  REQUIRE(cfg->every >= 1 && cfg->pool_rows >= 1, "dbmp_prune: every (%d) and pool_rows (%d) must be >= 1",
+          cfg->every, cfg->pool_rows);
+  REQUIRE(g.N == 0 || (pool && means2D && radii && rotations && opacities && colors), "dbmp_prune: null pointer");
+  PruneArgs a{cfg->every, cfg->num_iterations, cfg->no_prune_last, cfg->warmup, cfg->threshold, cfg->pool_rows};
+  return launch_prune(g, a, step_count, pool, state, means2D, radii, rotations, opacities, colors, skip_flag,
+                      (cudaStream_t)stream);
+}
+
+int dbmp_template_blur_scheduled(const float* templates, int P, int Ht, int Wt, const dbmp_blur_schedule* sched,
+                                 const int32_t* step_count, float* out, void* stream) {
+  REQUIRE(P >= 0 && Ht >= 1 && Wt >= 1, "dbmp_template_blur_scheduled: bad atlas shape %dx%dx%d", P, Ht, Wt);
+  REQUIRE(sched && step_count, "dbmp_template_blur_scheduled: null schedule / step_count");
+  REQUIRE(P == 0 || (templates && out && templates != out), "dbmp_template_blur_scheduled: null or in-place buffers");
+  REQUIRE(sched->mode >= 0 && sched->mode <= 2, "dbmp_template_blur_scheduled: mode %d unknown", sched->mode);
+  REQUIRE(sched->mode != 2 || sched->num_iterations >= 1, "dbmp_template_blur_scheduled: num_iterations must be >= 1");
+  return launch_template_blur_sched(templates, P, Ht, Wt, sched, step_count, out, (cudaStream_t)stream);
 }
 
 int dbmp_psd_bboxes(const float* means2D, const float* radii, int N, int H, int W, float scale, int32_t* out_bbox,

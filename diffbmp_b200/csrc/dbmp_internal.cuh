@@ -273,6 +273,22 @@ __device__ __forceinline__ float sigmoid_precise(float x) {
   return z / (1.f + z);
 }
 
+// Optimiser step arguments (dbmp_adam_cfg as the kernels take it).
+struct AdamArgs {
+  float lr[8];            // per parameter: x, y, r, theta, v, c_r, c_g, c_b
+  float beta1, beta2, eps;
+  float x_max, y_max, r_min, r_max;
+  int clamp;
+  float gamma;            // ExponentialLR factor per completed step (1: none)
+};
+
+// Pruning arguments (dbmp_prune_cfg).
+struct PruneArgs {
+  int every, num_iterations, no_last, warmup;
+  float threshold;
+  int pool_rows;
+};
+
 // Thread-local error string shared by every entry point.
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);

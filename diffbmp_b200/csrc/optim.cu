@@ -16,13 +16,6 @@ __device__ __forceinline__ double sigmoid_dd(double x) {
   return z / (1.0 + z);
 }
 
-struct AdamArgs {
-  float lr[8];            // per parameter: x, y, r, theta, v, c_r, c_g, c_b
-  float beta1, beta2, eps;
-  float x_max, y_max, r_min, r_max;
-  int clamp;
-};
-
 __global__ void adam_kernel(Geom g, AdamArgs a, const double* __restrict__ gacc, float* __restrict__ means2D,
                             float* __restrict__ radii, float* __restrict__ rot, float* __restrict__ opac,
                             float* __restrict__ colors, float* __restrict__ m1, float* __restrict__ m2,
@@ -31,6 +24,9 @@ __global__ void adam_kernel(Geom g, AdamArgs a, const double* __restrict__ gacc,
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= g.N) return;
   const int t = *step_count + 1;
+  // torch.optim.lr_scheduler.ExponentialLR stepped after every optimizer step:
+  // the t-th step runs with lr * gamma^(t-1) (simple_tile_renderer.py:1128-1129)
+  const double decay = a.gamma == 1.f ? 1.0 : pow((double)a.gamma, (double)(t - 1));
   const double bc1 = 1.0 - pow((double)a.beta1, (double)t);
   const double bc2s = sqrt(1.0 - pow((double)a.beta2, (double)t));
   // gradient chain (same as finalize_kernel)
@@ -66,7 +62,7 @@ __global__ void adam_kernel(Geom g, AdamArgs a, const double* __restrict__ gacc,
     vk = fmaf(a.beta2, vk, (1.f - a.beta2) * gk * gk);     // exp_avg_sq.mul_(beta2).addcmul_(g, g, 1-beta2)
     m1[(size_t)n * 8 + k] = mk;
     m2[(size_t)n * 8 + k] = vk;
-    const float step_size = (float)((double)a.lr[k] / bc1);
+    const float step_size = (float)((double)a.lr[k] * decay / bc1);
     const float denom = sqrtf(vk) / (float)bc2s + a.eps;
     *p[k] -= step_size * mk / denom;
   }
@@ -80,6 +76,77 @@ __global__ void adam_kernel(Geom g, AdamArgs a, const double* __restrict__ gacc,
 __global__ void step_increment_kernel(int* __restrict__ step_count, const int* __restrict__ skip_flag) {
   if (skip_flag != nullptr && *skip_flag != 0) return;
   *step_count += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Pruning (restart) of low-opacity primitives: the reference's do_prune
+// (simple_tile_renderer.py:1007-1013 schedule, :1236-1270 selection and
+// replacement) as one CTA.  Primitives with sigmoid(v) < threshold, in
+// ascending index order, take consecutive rows of the replacement pool; a
+// CTA-wide scan over chunks of kPruneThreads primitives gives each its rank.
+constexpr int kPruneThreads = 1024;
+
+__global__ void __launch_bounds__(kPruneThreads) prune_kernel(Geom g, PruneArgs a, const int* __restrict__ step_count,
+                                                              const float* __restrict__ pool, int* __restrict__ state,
+                                                              float* __restrict__ means2D, float* __restrict__ radii,
+                                                              float* __restrict__ rot, float* __restrict__ opac,
+                                                              float* __restrict__ colors,
+                                                              const int* __restrict__ skip_flag) {
+  __shared__ int s_warp[kPruneThreads / 32];
+  __shared__ int s_total;
+  if (skip_flag != nullptr && *skip_flag != 0) return;
+  const int it = *step_count;
+  // the reference's schedule (simple_tile_renderer.py:1007-1012); an iteration
+  // replayed after an overflowed binning is not pruned a second time
+  if (!(it != 0 && it % a.every == 0 && it < a.num_iterations - a.no_last && it > a.warmup) || state[1] == it)
+    return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int base = state[0];
+  int done = 0;
+  for (int c = 0; c < g.N; c += kPruneThreads) {
+    const int n = c + threadIdx.x;
+    // torch.sigmoid in float32: 1 / (1 + exp(-v)); compared with the threshold as float32
+    const bool low = n < g.N && (1.f / (1.f + expf(-opac[n]))) < a.threshold;
+    const unsigned m = __ballot_sync(0xffffffffu, low);
+    if (lane == 0) s_warp[warp] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0;
+      for (int w = 0; w < kPruneThreads / 32; ++w) { const int v = s_warp[w]; s_warp[w] = run; run += v; }
+      s_total = run;
+    }
+    __syncthreads();
+    if (low) {
+      const int rank = done + s_warp[warp] + __popc(m & ((1u << lane) - 1u));
+      const float* r = pool + (size_t)((base + rank) % a.pool_rows) * 8;
+      means2D[2 * n] = r[0];
+      means2D[2 * n + 1] = r[1];
+      radii[n] = r[2];
+      rot[n] = r[3];
+      opac[n] = r[4];
+      colors[3 * n] = r[5];
+      colors[3 * n + 1] = r[6];
+      colors[3 * n + 2] = r[7];
+    }
+    done += s_total;
+    __syncthreads();   // s_warp / s_total are rewritten by the next chunk
+  }
+  if (threadIdx.x == 0) {
+    state[0] = (int)(((long long)base + done) % a.pool_rows);
+    state[1] = it;
+    state[2] = done;
+    state[3] += done;
+  }
+}
+
+int launch_prune(const Geom& g, const PruneArgs& a, const int* step_count, const float* pool, int* state,
+                 float* means2D, float* radii, float* rot, float* opac, float* colors, const int* skip_flag,
+                 cudaStream_t st) {
+  if (g.N == 0) return DBMP_OK;
+  prune_kernel<<<1, kPruneThreads, 0, st>>>(g, a, step_count, pool, state, means2D, radii, rot, opac, colors,
+                                            skip_flag);
+  DBMP_CHECK_LAUNCH("prune_kernel");
+  return DBMP_OK;
 }
 
 int launch_adam(const Geom& g, const AdamArgs& a, const double* gacc, float* means2D, float* radii, float* rot,

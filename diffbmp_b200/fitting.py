@@ -27,8 +27,43 @@ from . import _lib
 from ._lib import AdamCfg, call, lib
 from .rasterizer import Atlas, Rasterizer, _ptr, _stream, DEFAULT_T_STOP
 
-# Reference defaults (pydiffbmp/util/constants.py:24-31): base lr and gains.
+# Reference defaults (pydiffbmp/util/constants.py:24-38): base lr and gains,
+# ExponentialLR factor, fixed blur sigma.
 LR_GAINS = dict(x=10.0, y=10.0, r=10.0, v=1.5, theta=1.0, c=1.0)
+DECAY_RATE = 0.99
+BLUR_SIGMA = 1.0
+BLUR_MODES = {"none": 0, "fixed": 1, "adaptive": 2}
+
+
+@dataclass
+class PruneConfig:
+    """The reference's pruning (restart) options, opt_conf["pruning"]
+    (simple_tile_renderer.py:980-981,1007-1013): every `every` iterations
+    inside (warmup, num_iterations - no_prune_last), primitives with
+    sigmoid(opacity) < threshold are re-initialised.  `pool` (R,8) holds the
+    replacement parameters (x, y, r, theta, opacity logit, colour logits) that
+    the reference draws from its initializer at each prune; rows are used in
+    order, cyclically (``fallback_pool`` draws them as the reference's
+    _fallback_random_init does)."""
+    pool: object
+    threshold: float = 0.3
+    every: int = 5
+    no_prune_last: int = 10
+    warmup: int = 20
+
+
+def fallback_pool(rng: np.random.Generator, H: int, W: int, rows: int) -> np.ndarray:
+    """Replacement rows drawn as the reference's _fallback_random_init
+    (simple_tile_renderer.py:1272-1282): x U[0,W), y U[0,H), r U[0,1) *
+    min(H,W)/20 + 2, opacity logit -2, theta U[0,2pi), colour logits U[0,1)."""
+    out = np.empty((rows, 8), np.float32)
+    out[:, 0] = rng.random(rows) * W
+    out[:, 1] = rng.random(rows) * H
+    out[:, 2] = rng.random(rows) * (min(H, W) / 20) + 2
+    out[:, 3] = rng.random(rows) * 2 * np.pi
+    out[:, 4] = -2.0
+    out[:, 5:8] = rng.random((rows, 3))
+    return out
 
 
 @dataclass
@@ -42,6 +77,83 @@ class FitConfig:
     t_stop: float = DEFAULT_T_STOP
     fused: bool = True
     headroom: float = 1.3
+    # the rest of the reference's loop (simple_tile_renderer.py:970-981):
+    num_iterations: int = 0          # iterations of the whole fit (blur / prune schedules)
+    decay_rate: float = 1.0          # ExponentialLR gamma (do_decay: DECAY_RATE); 1: no decay
+    blur: str = "none"               # "fixed" (do_gaussian_blur) or "adaptive" (do_adapt_gaussian_blur)
+    blur_sigma: float = BLUR_SIGMA
+    blur_sigma_start: float = 2.0
+    blur_sigma_end: float = 0.0
+    prune: PruneConfig | None = None
+
+    @classmethod
+    def from_opt_conf(cls, opt_conf: dict, pool=None, **over) -> "FitConfig":
+        """The settings of the reference's optimisation config (the
+        "optimization" block read by _optimize_parameters_whole,
+        simple_tile_renderer.py:939-981): learning_rate.default and gains,
+        num_iterations, do_decay / decay_rate, do_gaussian_blur / blur_sigma,
+        do_adapt_gaussian_blur / blur_sigma_start / blur_sigma_end and pruning.
+        Pruning needs `pool`, the replacement rows of PruneConfig."""
+        lr_conf = opt_conf.get("learning_rate", {})
+        gains = dict(LR_GAINS)
+        for k in ("x", "y", "r", "v", "theta", "c"):
+            gains[k] = float(lr_conf.get(f"gain_{k}", gains[k]))
+        blur = "adaptive" if opt_conf.get("do_adapt_gaussian_blur") else \
+            "fixed" if opt_conf.get("do_gaussian_blur") else "none"
+        pr = opt_conf.get("pruning", {})
+        prune = None
+        if pr.get("do_pruning", False):
+            if pool is None:
+                raise ValueError("pruning needs the replacement pool (PruneConfig.pool)")
+            prune = PruneConfig(pool, float(pr.get("prune_threshold", 0.3)), int(pr.get("prune_iterations", 5)),
+                                int(pr.get("no_prune_last_iterations", 10)),
+                                int(pr.get("no_prune_warmup_iterations", 20)))
+        kw = dict(lr=float(lr_conf.get("default", 0.1)), gains=gains,
+                  num_iterations=int(opt_conf.get("num_iterations", 100)),
+                  decay_rate=float(opt_conf.get("decay_rate", DECAY_RATE)) if opt_conf.get("do_decay") else 1.0,
+                  blur=blur, blur_sigma=float(opt_conf.get("blur_sigma", BLUR_SIGMA)),
+                  blur_sigma_start=float(opt_conf.get("blur_sigma_start", 2.0)),
+                  blur_sigma_end=float(opt_conf.get("blur_sigma_end", 0.0)), prune=prune)
+        kw.update(over)
+        return cls(**kw)
+
+
+# Host statements of the loop's schedules; the device kernels (dbmp_adam_step,
+# dbmp_template_blur_scheduled, dbmp_prune) evaluate the same expressions from
+# the device step count.
+def lr_schedule(cfg: FitConfig, N: int, it: int) -> list:
+    """Learning rates of the reference's Adam groups (x, y, r, v, theta, c) at
+    iteration it: lr * gain (v: * 1000/N) * decay_rate^it
+    (simple_tile_renderer.py:961-973, ExponentialLR stepped once per iteration)."""
+    g, d = cfg.gains, cfg.decay_rate ** it
+    return [cfg.lr * g["x"] * d, cfg.lr * g["y"] * d, cfg.lr * g["r"] * d,
+            cfg.lr * g["v"] * (1000.0 / max(N, 1)) * d, cfg.lr * g["theta"] * d, cfg.lr * g["c"] * d]
+
+
+def blur_sigma_at(cfg: FitConfig, it: int) -> float:
+    """Template blur sigma of iteration it (simple_tile_renderer.py:1015-1022)."""
+    if cfg.blur == "adaptive":
+        progress = it / cfg.num_iterations
+        return cfg.blur_sigma_start * (1 - progress) + cfg.blur_sigma_end * progress
+    if cfg.blur == "fixed":
+        return cfg.blur_sigma
+    return 0.0
+
+
+def prune_due(cfg: FitConfig, it: int) -> bool:
+    """Whether iteration it prunes (simple_tile_renderer.py:1007-1012)."""
+    p = cfg.prune
+    return (p is not None and it != 0 and it % p.every == 0 and it < cfg.num_iterations - p.no_prune_last
+            and it > p.warmup)
+
+
+def prune_selection(cfg: FitConfig, opacity_logits) -> np.ndarray:
+    """Indices the prune replaces: sigmoid(v) < threshold in float32
+    (simple_tile_renderer.py:1244-1254), ascending."""
+    v = np.asarray(opacity_logits, np.float32)
+    with np.errstate(over="ignore"):
+        sig = (np.float32(1) / (np.float32(1) + np.exp(-v))).astype(np.float32)
+    return np.nonzero(sig < np.float32(cfg.prune.threshold))[0]
 
 
 def _upload(a: np.ndarray, device) -> torch.Tensor:
@@ -118,7 +230,33 @@ class ImageFitter:
         lrs = [lr * g["x"], lr * g["y"], lr * g["r"], lr * g["theta"], lr * g["v"] * (1000.0 / max(self.N, 1))] + \
               [lr * g["c"]] * 3
         self.adam_cfg = AdamCfg((ctypes.c_float * 8)(*lrs), cfg.betas[0], cfg.betas[1], cfg.eps,
-                                float(self.W - 1), float(self.H - 1), 2.0, float(min(self.H, self.W) // 4), 1)
+                                float(self.W - 1), float(self.H - 1), 2.0, float(min(self.H, self.W) // 4), 1,
+                                float(cfg.decay_rate))
+        # blur schedule: the job re-blurs the atlas's templates into its own
+        # texel buffer every step (the content bboxes stay the unblurred ones)
+        self.blur = None
+        if cfg.blur != "none":
+            if cfg.blur not in BLUR_MODES:
+                raise ValueError(f"blur must be one of {sorted(BLUR_MODES)}, not {cfg.blur!r}")
+            if cfg.blur == "adaptive" and cfg.num_iterations < 1:
+                raise ValueError("the adaptive blur schedule needs FitConfig.num_iterations")
+            self.atlas = atlas.private_copy()
+            self.cv = self.rz.canvas(self.N, self.atlas)
+            self.blur = _lib.BlurSchedule(BLUR_MODES[cfg.blur], cfg.blur_sigma, cfg.blur_sigma_start,
+                                          cfg.blur_sigma_end, int(cfg.num_iterations))
+            self._blurred = (self.atlas.data if self.atlas.kind == _lib.ATLAS_F32
+                             else torch.empty_like(self.atlas.templates))
+            self._blur_step()     # this iteration's texels before the first binning / render
+        self.prune = None
+        if cfg.prune is not None:
+            pc = cfg.prune
+            if cfg.num_iterations < 1:
+                raise ValueError("pruning needs FitConfig.num_iterations")
+            pool = pc.pool if isinstance(pc.pool, torch.Tensor) else torch.from_numpy(np.asarray(pc.pool, np.float32))
+            self.prune_pool = pool.to(device=dev, dtype=torch.float32).contiguous().view(-1, 8)
+            self.prune_state = torch.zeros(4, dtype=torch.int32, device=dev)
+            self.prune = _lib.PruneCfg(int(pc.every), int(cfg.num_iterations), int(pc.no_prune_last),
+                                       int(pc.warmup), float(pc.threshold), int(self.prune_pool.shape[0]))
         self.steps_enqueued = 0
         self.graph = None
         self._host_state = None   # pinned (step count, loss) staged by stage_result()
@@ -150,12 +288,29 @@ class ImageFitter:
                 _ptr(self.colors), _ptr(self.sel)]
 
     # -- one iteration -------------------------------------------------------
+    def _blur_step(self, st=None):
+        """This iteration's blurred texels (blur schedule on the device step count)."""
+        st = st if st is not None else _stream()
+        a = self.atlas
+        call("dbmp_template_blur_scheduled", _ptr(a.templates), a.P, a.Ht, a.Wt, ctypes.byref(self.blur),
+             _ptr(self.step_count), _ptr(self._blurred), st)
+        if a.kind != _lib.ATLAS_F32:
+            call("dbmp_atlas_pack", _ptr(self._blurred), a.P, a.Ht, a.Wt, a.kind, _ptr(a.data), st)
+
     def _enqueue(self):
         st = _stream()
         cv = self.cv
         rz = self.rz
         ws, wsb = rz._ws_ptr()
         skip = ctypes.c_void_p(self.flags.data_ptr() + 4)
+        # the reference's iteration order: prune, blur, render, loss, backward,
+        # Adam step, lr decay, clamp (simple_tile_renderer.py:1003-1131)
+        if self.prune is not None:
+            call("dbmp_prune", ctypes.byref(cv), ctypes.byref(self.prune), _ptr(self.step_count),
+                 _ptr(self.prune_pool), _ptr(self.prune_state), _ptr(self.means2D), _ptr(self.radii),
+                 _ptr(self.rotations), _ptr(self.opacities), _ptr(self.colors), None, st)
+        if self.blur is not None:
+            self._blur_step(st)
         call("dbmp_bin", ctypes.byref(cv), *self._param_ptrs(), _ptr(self.atlas.bbox), _ptr(self.prim_info),
              _ptr(self.offsets), _ptr(rz._idx), ctypes.c_longlong(rz.capacity), _ptr(self.flags), skip, ws,
              ctypes.c_size_t(wsb), st)

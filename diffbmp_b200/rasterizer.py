@@ -81,6 +81,16 @@ class Atlas:
             self.data = torch.empty(nbytes, dtype=torch.uint8, device=t.device)
             call("dbmp_atlas_pack", _ptr(self.templates), self.P, self.Ht, self.Wt, self.kind, _ptr(self.data), st)
 
+    def private_copy(self) -> "Atlas":
+        """An atlas of the same kind, templates and content bboxes with its own
+        texel buffer (filled by the caller), for a job that re-derives its
+        texels every step (the fit loop's blur schedule)."""
+        a = Atlas.__new__(Atlas)
+        a.templates, a.sigma, a.bbox = self.templates, self.sigma, self.bbox
+        a.P, a.Ht, a.Wt, a.kind = self.P, self.Ht, self.Wt, self.kind
+        a.data = torch.empty_like(self.data)
+        return a
+
     def with_kind(self, kind) -> "Atlas":
         a = Atlas(self.templates, kind)
         a.bbox, a.sigma = self.bbox, self.sigma   # keep the unblurred content bboxes

@@ -189,8 +189,9 @@ int dbmp_backward(const dbmp_canvas* cv, const void* prim_info, const void* atla
  * dbmp_backward, but the (N,8) f64 gradient-sum scratch is a fixed array
  * inside this library's device module, so there is no grad_accum argument.
  * Limit: N <= dbmp_backward_noalloc_max_prims() (65536); larger N returns
- * DBMP_ERR_CAPACITY.  The array takes 4 MiB on every GPU that loads the
- * library, until exit.  The first call on a device looks up the array's
+ * DBMP_ERR_CAPACITY.  The array takes 4 MiB on every GPU that loads it
+ * (under CUDA's default lazy module loading, at the first call of this entry
+ * point on that GPU), until exit.  The first call on a device looks up the array's
  * device address with that device current, and a call after that device's
  * context changed (cudaDeviceReset) looks it up again: make the first call
  * on each device, and the first after a reset, before any stream capture.  All calls share the array (zeroed by each call), so calls that
@@ -285,6 +286,11 @@ typedef struct {
   float beta1, beta2, eps;
   float x_max, y_max, r_min, r_max;
   int32_t clamp;          /* 1: clamp x, y, r after the step */
+  float lr_gamma;         /* ExponentialLR factor: the step after k completed
+                             steps uses lr * lr_gamma^k (torch's
+                             ExponentialLR stepped after every optimizer step,
+                             simple_tile_renderer.py:970-973,1128-1129);
+                             0 or 1: no decay */
 } dbmp_adam_cfg;
 
 /* In-place Adam step of every primitive parameter from the raw sums in
@@ -298,6 +304,50 @@ int dbmp_adam_step(const dbmp_canvas* cv, const dbmp_adam_cfg* cfg, const double
                    float* means2D, float* radii, float* rotations, float* opacities, float* colors,
                    float* adam_m, float* adam_v, int32_t* step_count, const int32_t* skip_flag,
                    void* stream);
+
+/* Pruning (restart) of low-opacity primitives, the reference's do_prune
+ * (simple_tile_renderer.py:1007-1013,1236-1270) on the device.  At iteration
+ * it = *step_count (completed steps), when it != 0, it % every == 0,
+ * it < num_iterations - no_prune_last and it > warmup, every primitive with
+ * sigmoid(opacity) < threshold (float32 sigmoid, as torch.sigmoid) takes the
+ * next row of `pool` ((pool_rows, 8) f32: x, y, r, theta, opacity logit,
+ * colour logits r, g, b -- the replacement parameters an initializer drew,
+ * used in ascending primitive order, cyclically); Adam moments are kept, as
+ * in the reference.  state (4 device int32, zeroed by the caller before the
+ * first step): [0] next pool row, [1] iteration of the last prune (a replayed
+ * iteration is not pruned twice), [2] primitives replaced by the last prune,
+ * [3] primitives replaced in total.  skip_flag as in dbmp_adam_step.  One
+ * single-CTA launch; other iterations return at once. */
+typedef struct {
+  int32_t every;            /* prune_iterations */
+  int32_t num_iterations;   /* iterations of the fit */
+  int32_t no_prune_last;    /* no_prune_last_iterations */
+  int32_t warmup;           /* no_prune_warmup_iterations */
+  float threshold;          /* prune_threshold on sigmoid(opacity) */
+  int32_t pool_rows;        /* rows of pool (>= 1) */
+} dbmp_prune_cfg;
+int dbmp_prune(const dbmp_canvas* cv, const dbmp_prune_cfg* cfg, const int32_t* step_count,
+               const float* pool, int32_t* state, float* means2D, float* radii, float* rotations,
+               float* opacities, float* colors, const int32_t* skip_flag, void* stream);
+
+/* Blur schedule of the fit loop (simple_tile_renderer.py:975-979,1015-1021):
+ * at iteration it = *step_count the templates are blurred with
+ * mode 0: sigma 0 (unchanged); mode 1: `sigma` (do_gaussian_blur);
+ * mode 2: sigma_start (1 - it/num_iterations) + sigma_end it/num_iterations
+ * (do_adapt_gaussian_blur), evaluated in double as the reference does, then
+ * as dbmp_template_blur (kernel size from the double sigma, weights in
+ * float).  The reference's CPU path blurs its templates per iteration this
+ * way (simple_tile_renderer.py:1499-1505); its CUDA path does not read the
+ * per-iteration sigma at all (TileConfig.sigma, cuda_kernels/tile_common.h:28,
+ * is unused by the kernels), which mode 0 reproduces. */
+typedef struct {
+  int32_t mode;
+  float sigma, sigma_start, sigma_end;
+  int32_t num_iterations;
+} dbmp_blur_schedule;
+int dbmp_template_blur_scheduled(const float* templates, int P, int Ht, int Wt,
+                                 const dbmp_blur_schedule* sched, const int32_t* step_count, float* out,
+                                 void* stream);
 
 /* PSD stage 1: crop box per primitive, [x0,y0,x1,y1) of the square of half
  * extent 1.5*r*scale around means2D*scale, clipped to the HxW export canvas;

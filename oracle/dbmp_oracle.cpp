@@ -55,7 +55,8 @@ struct Scene {
   int sem;
   double t_stop;          // 0 disables early termination (reference behaviour)
   double edge;            // boundary shift: > 0 widens the cull and the texel cut
-                          // by `edge` (pixels / texels), < 0 narrows them; tests
+                          // by `edge` (pixels / texels), < 0 narrows them, and
+                          // the bilinear cell choice moves by 2 float32 ulps; tests
                           // use +-edge renders to find boundary-sensitive pixels
   const double* cmap = nullptr;   // (N,Ht,Wt,3) colour maps (colors_orig), or null
   double cblend = 0.0;            // colour-map blend weight (used when cmap && cblend > 0)
@@ -78,7 +79,18 @@ inline double sample_tmpl(const double* t, int Ht, int Wt, double x, double y,
       return 0.0;
     }
   }
-  double fx = std::floor(x), fy = std::floor(y);
+  // The bilinear cell is the one left of / above (x, y); its gradient jumps
+  // across texel grid lines (the value does not), and a float32 texel
+  // coordinate within its rounding of a line can fall on either side.  The
+  // +-edge band runs therefore also move the cell choice by two float32 ulps
+  // of the coordinate, so that both one-sided gradients of such points
+  // appear in the band's spread.
+  auto cell_shift = [&](double v) {
+    if (edge == 0.0 || !std::isfinite(v)) return 0.0;
+    const double ulp = std::ldexp(1.0, std::max(std::ilogb(std::max(std::fabs(v), 1.0)), -126) - 23);
+    return std::copysign(2.0 * ulp, edge);
+  };
+  double fx = std::floor(x + cell_shift(x)), fy = std::floor(y + cell_shift(y));
   if (!std::isfinite(fx) || !std::isfinite(fy) || fx < -2.0 || fy < -2.0 ||
       fx > (double)Wt + 1.0 || fy > (double)Ht + 1.0) {
     if (gx) { *gx = 0; *gy = 0; }

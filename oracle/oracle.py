@@ -223,8 +223,10 @@ def psd_layers(means2D, radii, rot, colors_sig, vis_sig, templates, sel, bboxes,
 
 def boundary_band(scene: Scene, offs, idx, edge=1e-3, t_stop=0.0, nthreads=0):
     """Per-pixel spread of the image between renders whose cull and texel-cut
-    boundaries are widened and narrowed by `edge`: non-zero where a float
-    rounding difference at a primitive's boundary can flip a fragment.
+    boundaries are widened and narrowed by `edge` (and whose bilinear cell
+    choice moves by two float32 ulps of the texel coordinate, where the
+    bilinear gradient jumps): non-zero where a float rounding difference
+    at a primitive's boundary can flip a fragment.
     Returns (spread_color (H,W), spread_alpha (H,W))."""
     hi = forward(scene, offs, idx, SEM_KERNEL, t_stop, nthreads, edge=+edge)
     lo = forward(scene, offs, idx, SEM_KERNEL, t_stop, nthreads, edge=-edge)
@@ -253,8 +255,10 @@ def check_image(scene: Scene, offs, idx, color, alpha, tol=1e-5, ref=None, nthre
 def check_grads(scene: Scene, offs, idx, grad_color, grad_alpha, ours, rel=1e-4, nthreads=0, verbose=True):
     """Per parameter block k of the (N,8) gradients:
     ||ours - oracle|| <= rel ||oracle|| + ||oracle(+edge) - oracle(-edge)||
-    (the band spread of the gradient, edge = 1e-3).  Returns the per-block
-    relative errors."""
+    (the band spread of the gradient, edge = 1e-3: fragments within 1e-3 of
+    the cull square or the texel cut, and points within two float32 ulps of
+    a texel grid line, where the bilinear gradient jumps).  Returns the
+    per-block relative errors."""
     ref = backward(scene, offs, idx, grad_color, grad_alpha, nthreads=nthreads)
     hi = backward(scene, offs, idx, grad_color, grad_alpha, nthreads=nthreads, edge=1e-3)
     lo = backward(scene, offs, idx, grad_color, grad_alpha, nthreads=nthreads, edge=-1e-3)

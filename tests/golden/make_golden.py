@@ -24,6 +24,7 @@ the code paths exercised below.  Fixtures produced:
 from __future__ import annotations
 
 import argparse
+import json
 import importlib.abc
 import importlib.machinery
 import os
@@ -152,12 +153,116 @@ def gen_torch_case(str_, name, H, W, ts, S, N, seed, rmin, rmax, amax):
     print(f"torch_{name}: N={N} image sum={float(img.sum()):.4f}")
 
 
+# Options of the recorded fit loop: ExponentialLR decay, the adaptive blur
+# schedule and pruning, as the reference's opt_conf names them.
+FIT_LOOP_CONF = {
+    "num_iterations": 50,
+    "learning_rate": {"default": 0.01, "gain_x": 10.0, "gain_y": 10.0, "gain_r": 10.0, "gain_v": 1.5,
+                      "gain_theta": 1.0, "gain_c": 1.0},
+    "loss_config": {"type": "mse"},
+    "do_decay": True, "decay_rate": 0.95,
+    "do_adapt_gaussian_blur": True, "blur_sigma_start": 2.0, "blur_sigma_end": 0.0,
+    "pruning": {"do_pruning": True, "prune_iterations": 5, "no_prune_last_iterations": 10,
+                "no_prune_warmup_iterations": 20, "prune_threshold": 0.3},
+    "bg_color": "white",
+}
+
+
+def gen_fit_loop(str_):
+    """Runs the reference's optimisation loop (SimpleTileRenderer.
+    _optimize_parameters_whole, simple_tile_renderer.py:913-1228) on its CPU
+    path for the 256x256 / N=512 soft-disk scene with FIT_LOOP_CONF, and
+    records per iteration the learning rate of each Adam parameter group at
+    its step, the blur sigma handed to the renderer, and each prune: its
+    iteration, the opacity logits it saw and the primitives it replaced.  The
+    initializer is a stand-in whose reinitialize_subset hands out consecutive
+    rows of a seeded pool (the reference's own initializers are outside this
+    path)."""
+    import tempfile
+    import torch
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.fitting import fallback_pool
+    s = wl.make_scene("c0", 0)
+    N = s.N
+    pool = fallback_pool(np.random.default_rng(17), s.H, s.W, 4 * N)
+    R = make_renderer(str_, s.H, s.W, s.templates, 32, 1.0)
+    R.output_path = tempfile.mkdtemp()
+    str_.vram_used_by_pid = lambda pid=None: 0          # NVML is absent on this host
+    rec = dict(lrs=[], sigmas=[], prune_its=[], prune_v=[], prune_idx=[])
+    orig_step = torch.optim.Adam.step
+
+    def step(self, *a, **k):
+        rec["lrs"].append([g["lr"] for g in self.param_groups])
+        return orig_step(self, *a, **k)
+    orig_render = R.render_from_params
+
+    def render(*a, **k):
+        rec["sigmas"].append(float(k.get("sigma", 0.0)))
+        # render_from_params picks the per-tile path only when torch sees a GPU
+        # (simple_tile_renderer.py:249); its sequential CPU path does not run as
+        # written, so the per-tile path (CPU fallback inside) is forced here
+        real = torch.cuda.is_available
+        torch.cuda.is_available = lambda: True
+        try:
+            return orig_render(*a, **k)
+        finally:
+            torch.cuda.is_available = real
+    orig_prune = R.do_prune
+
+    def do_prune(x, y, r, v, theta, c, prune_conf, initializer, target_image):
+        v0 = v.detach().clone()
+        x0 = x.detach().clone()
+        orig_prune(x, y, r, v, theta, c, prune_conf, initializer, target_image)
+        rec["prune_its"].append(len(rec["sigmas"]))
+        rec["prune_v"].append(v0.numpy())
+        rec["prune_idx"].append(np.nonzero((x.detach() != x0).numpy() | (v.detach() != v0).numpy())[0])
+
+    class Initializer:
+        decrease_max_radius = 0
+
+        def __init__(self):
+            self.cursor = 0
+
+        def reinitialize_subset(self, n, target, device):
+            rows = torch.from_numpy(pool[[(self.cursor + i) % len(pool) for i in range(n)]])
+            self.cursor += n
+            return (rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 4], rows[:, 3], rows[:, 5:8])
+
+    R.render_from_params = render
+    R.do_prune = do_prune
+    torch.optim.Adam.step = step
+    try:
+        leaf = lambda a: torch.tensor(np.ascontiguousarray(a), requires_grad=True)
+        x, y = leaf(s.means2D[:, 0]), leaf(s.means2D[:, 1])
+        r, th, v, c = leaf(s.radii), leaf(s.rotations), leaf(s.opacities), leaf(s.colors)
+        import copy
+        R._optimize_parameters_whole(x, y, r, v, th, c, torch.from_numpy(s.target), copy.deepcopy(FIT_LOOP_CONF),
+                                     initializer=Initializer())
+    finally:
+        torch.optim.Adam.step = orig_step
+    idx = np.concatenate(rec["prune_idx"]) if rec["prune_idx"] else np.zeros(0, np.int64)
+    np.savez_compressed(
+        os.path.join(HERE, "fit_loop.npz"), N=N, lrs=np.array(rec["lrs"], np.float64),
+        sigmas=np.array(rec["sigmas"], np.float64), prune_its=np.array(rec["prune_its"], np.int64),
+        prune_v=np.stack(rec["prune_v"]) if rec["prune_v"] else np.zeros((0, N), np.float32),
+        prune_counts=np.array([len(i) for i in rec["prune_idx"]], np.int64), prune_idx=idx.astype(np.int64),
+        pool=pool, conf=json.dumps(FIT_LOOP_CONF), decay_rate=FIT_LOOP_CONF["decay_rate"], sigma_start=FIT_LOOP_CONF["blur_sigma_start"],
+        sigma_end=FIT_LOOP_CONF["blur_sigma_end"], iterations=FIT_LOOP_CONF["num_iterations"],
+        final=np.concatenate([t.detach().numpy().reshape(N, -1) for t in (x, y, r, th, v, c)], 1))
+    print(f"fit_loop: {len(rec['lrs'])} steps, prunes at {rec['prune_its']} replacing "
+          f"{[len(i) for i in rec['prune_idx']]}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DIFFBMP_REFERENCE"),
                     help="root of the reference checkout (or set DIFFBMP_REFERENCE)")
+    ap.add_argument("--only", default=None, help="regenerate one fixture group only (e.g. fit_loop)")
     args = ap.parse_args()
     str_ = load_reference(args.reference)
+    if args.only == "fit_loop":
+        gen_fit_loop(str_)
+        return
     from diffbmp_b200 import workloads as wl
     import torch
 
@@ -195,6 +300,8 @@ def main():
     gen_torch_case(str_, "ragged", 80, 96, 16, atlas_ns, 48, 22, 3.0, 25.0, 0.8)
     torch.set_num_threads(1)
     gen_blur(args.reference)
+    torch.set_num_threads(os.cpu_count() or 1)
+    gen_fit_loop(str_)
 
 
 def gen_blur(ref_root):

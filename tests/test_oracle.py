@@ -190,3 +190,28 @@ def test_finite_difference_gradcheck_fp64():
         ok = ~np.isnan(fd)
         assert rel_err(g[ok, k], fd[ok], floor=1e-9) < 1e-5, f"block {k} ({name})"
     assert checked >= 8 * sc.N - 8, (checked, skipped)
+
+
+def test_band_covers_texel_grid_lines():
+    """A point 1e-7 texel below a texel grid line: float32 can round its
+    coordinate onto the line, where the bilinear gradient jumps (the value
+    does not).  The +-edge band runs give its two one-sided gradients, the
+    plain run one of them, and the image does not move."""
+    from diffbmp_b200 import workloads as wl
+    T = wl.random_shape(np.random.default_rng(4), 32)[None]
+    hy, r, py = 15.5, 10.0, 20
+    my = py - r * ((10.0 - 1e-7) / hy - 1.0)          # texel row of pixel row py: 10 - 1e-7
+    # centre x 17.3: no pixel of row py lies on the cull square or the texel cut
+    sc = O.Scene(40, 40, 32, np.array([[17.3, my]]), np.array([r]), np.array([0.0]), np.array([2.0]),
+                 np.zeros((1, 3)), T, np.zeros(1, np.int32))
+    offs, idx = bin_scene(sc, O.BIN_CULL)
+    gc = np.zeros((40, 40, 3), np.float32)
+    gc[py, :, :] = 1.0                                  # only row py carries gradient
+    g0 = O.backward(sc, offs, idx, gc, None)
+    hi = O.backward(sc, offs, idx, gc, None, edge=1e-3)
+    lo = O.backward(sc, offs, idx, gc, None, edge=-1e-3)
+    assert np.abs(hi - lo)[0, 1] > 1e-3 * np.abs(g0[0, 1])        # the y-gradient jumps across the line
+    assert np.allclose(g0, lo) or np.allclose(g0, hi)
+    f0, fh, fl = (O.forward(sc, offs, idx, edge=e)["color"][py] for e in (0.0, 1e-3, -1e-3))
+    inner = slice(10, 25)                               # pixels away from the cull / cut edges
+    assert np.allclose(f0[inner], fh[inner], atol=1e-9) and np.allclose(f0[inner], fl[inner], atol=1e-9)

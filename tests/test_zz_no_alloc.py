@@ -54,14 +54,17 @@ def test_noalloc_backward_matches_backward_twice():
     spec = wl.make_scene("c1", seed=5, H=192, W=224, N=500)
     p, atlas, rz, state = _inputs(spec)
     ref = rz.backward(state, p["gc"], p["ga"], p["radii"], p["rot"], p["opac"], p["col"], atlas)  # allocating form
-    outs = [_outputs(spec.N) for _ in range(2)]
+    outs = [_outputs(spec.N) for _ in range(3)]
+    # the first call loads the library's device module (lazily, under CUDA's
+    # default lazy loading), which commits the fixed array's 4 MiB; the calls
+    # after it take no device memory (any allocation is at least 2 MiB)
+    _noalloc(p, atlas, rz, state, outs[0])
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
-    for o in outs:                                              # two calls in a row share the array
+    for o in outs[1:]:                                          # two more calls in a row share the array
         _noalloc(p, atlas, rz, state, o)
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
-    # no device memory is taken by the calls (any allocation is at least 2 MiB)
     assert free0 - free1 < (1 << 20), (free0, free1)
     for o in outs:
         for a, b in zip(o, ref):
