@@ -78,6 +78,8 @@ SIGNATURES = {
     "dbmp_psd_rle_write": (_i, [_vp] * 4 + [_i, _ll, _i, _i] + [_vp] * 4 + [_ll, _vp]),
     "dbmp_count": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_fused_fwd_bwd": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_forward_batch": (_i, [_CP, _i, _vp, _vp, _vp, _vp, _ll, _vp, _ll, _f, _vp, _vp, _vp, _vp, _vp]),
+    "dbmp_backward_batch": (_i, [_CP, _i, _vp, _vp, _vp, _vp, _ll, _vp, _ll, _f] + [_vp] * 15),
     "dbmp_grads_from_accum": (_i, [_CP] + [_vp] * 11),
     "dbmp_prune": (_i, [_CP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dbmp_template_blur_scheduled": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp]),

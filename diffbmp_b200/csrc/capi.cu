@@ -37,10 +37,11 @@ int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* a
                    const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st);
 int launch_forward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                          const int* idx, float* color, float* alpha, float* T_last, int* last_pos, const float* cmap,
-                         float cblend, cudaStream_t st);
+                         float cblend, cudaStream_t st, int batch, long long idx_stride, long long cmap_stride);
 int launch_backward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                           const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
-                          const float* grad_alpha, double* gacc, const float* cmap, float cblend, cudaStream_t st);
+                          const float* grad_alpha, double* gacc, const float* cmap, float cblend, cudaStream_t st,
+                          int batch, long long idx_stride, long long cmap_stride);
 int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
                  unsigned long long* cnt, cudaStream_t st);
 int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
@@ -270,7 +271,8 @@ int dbmp_forward_blend(const dbmp_canvas* cv, const void* prim_info, const void*
   REQUIRE(c_blend >= 0.f && c_blend <= 1.f, "dbmp_forward_blend: c_blend %g outside [0, 1]", (double)c_blend);
   REQUIRE(c_blend == 0.f || g.N == 0 || colors_orig, "dbmp_forward_blend: colors_orig is null with c_blend > 0");
   return launch_forward_blend(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices,
-                              out_color, out_alpha, T_last, last_pos, colors_orig, c_blend, (cudaStream_t)stream);
+                              out_color, out_alpha, T_last, last_pos, colors_orig, c_blend, (cudaStream_t)stream, 1,
+                              0, 0);
 }
 
 int dbmp_backward_blend(const dbmp_canvas* cv, const void* prim_info, const void* atlas, const int32_t* tile_offsets,
@@ -295,9 +297,64 @@ int dbmp_backward_blend(const dbmp_canvas* cv, const void* prim_info, const void
     if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(grad_accum)");
   }
   rc = launch_backward_blend(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices,
-                             T_last, last_pos, grad_color, grad_alpha, grad_accum, colors_orig, c_blend, st);
+                             T_last, last_pos, grad_color, grad_alpha, grad_accum, colors_orig, c_blend, st, 1, 0, 0);
   if (rc) return rc;
   return launch_finalize(g, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
+                         grad_rotations, grad_opacities, grad_colors, st);
+}
+
+int dbmp_forward_batch(const dbmp_canvas* cv, int batch, const void* prim_info, const void* atlas,
+                       const int32_t* tile_offsets, const int32_t* tile_indices, long long index_stride,
+                       const float* colors_orig, long long colors_orig_stride, float c_blend, float* out_color,
+                       float* out_alpha, float* T_last, int32_t* last_pos, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_forward_batch");
+  if (rc) return rc;
+  REQUIRE(batch >= 0, "dbmp_forward_batch: batch %d < 0", batch);
+  REQUIRE(index_stride >= 0 && colors_orig_stride >= 0, "dbmp_forward_batch: negative stride");
+  REQUIRE(batch == 0 || (atlas && tile_offsets && tile_indices && out_color && out_alpha && T_last && last_pos),
+          "dbmp_forward_batch: null pointer");
+  REQUIRE(batch == 0 || g.N == 0 || prim_info, "dbmp_forward_batch: prim_info is null");
+  REQUIRE(c_blend >= 0.f && c_blend <= 1.f, "dbmp_forward_batch: c_blend %g outside [0, 1]", (double)c_blend);
+  REQUIRE(c_blend == 0.f || g.N == 0 || colors_orig, "dbmp_forward_batch: colors_orig is null with c_blend > 0");
+  REQUIRE(((uintptr_t)prim_info & 15) == 0, "dbmp_forward_batch: prim_info must be 16-byte aligned");
+  return launch_forward_blend(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices,
+                              out_color, out_alpha, T_last, last_pos, colors_orig, c_blend, (cudaStream_t)stream,
+                              batch, index_stride, colors_orig_stride);
+}
+
+int dbmp_backward_batch(const dbmp_canvas* cv, int batch, const void* prim_info, const void* atlas,
+                        const int32_t* tile_offsets, const int32_t* tile_indices, long long index_stride,
+                        const float* colors_orig, long long colors_orig_stride, float c_blend, const float* T_last,
+                        const int32_t* last_pos, const float* grad_color, const float* grad_alpha,
+                        const float* radii, const float* rotations, const float* opacities, const float* colors,
+                        double* grad_accum, float* grad_means2D, float* grad_radii, float* grad_rotations,
+                        float* grad_opacities, float* grad_colors, void* stream) {
+  Geom g;
+  int rc = make_geom(cv, &g, "dbmp_backward_batch");
+  if (rc) return rc;
+  REQUIRE(batch >= 0, "dbmp_backward_batch: batch %d < 0", batch);
+  REQUIRE(index_stride >= 0 && colors_orig_stride >= 0, "dbmp_backward_batch: negative stride");
+  REQUIRE(batch == 0 || (atlas && tile_offsets && tile_indices && T_last && last_pos && grad_color),
+          "dbmp_backward_batch: null input");
+  const bool work = batch > 0 && g.N > 0;
+  REQUIRE(!work || (prim_info && radii && rotations && opacities && colors), "dbmp_backward_batch: null parameter");
+  REQUIRE(!work || (grad_accum && grad_means2D && grad_radii && grad_rotations && grad_opacities && grad_colors),
+          "dbmp_backward_batch: null output");
+  REQUIRE(c_blend >= 0.f && c_blend <= 1.f, "dbmp_backward_batch: c_blend %g outside [0, 1]", (double)c_blend);
+  REQUIRE(c_blend == 0.f || g.N == 0 || colors_orig, "dbmp_backward_batch: colors_orig is null with c_blend > 0");
+  if (!work) return DBMP_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(grad_accum, 0, sizeof(double) * 8 * (size_t)g.N * batch, st);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync(grad_accum)");
+  rc = launch_backward_blend(g, cv->atlas_kind, (const PrimInfo*)prim_info, atlas, tile_offsets, tile_indices,
+                             T_last, last_pos, grad_color, grad_alpha, grad_accum, colors_orig, c_blend, st, batch,
+                             index_stride, colors_orig_stride);
+  if (rc) return rc;
+  // the chain rule is per primitive: the batch's (B, N) primitives are one flat array
+  Geom gb = g;
+  gb.N = g.N * batch;
+  return launch_finalize(gb, radii, rotations, opacities, colors, grad_accum, grad_means2D, grad_radii,
                          grad_rotations, grad_opacities, grad_colors, st);
 }
 

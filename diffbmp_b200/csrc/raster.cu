@@ -897,14 +897,23 @@ template <int TS, int KIND, bool CB>
 __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS, KIND, CB>()) forward_kernel(
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, float* __restrict__ out_color, float* __restrict__ out_alpha,
-    float* __restrict__ T_last, int* __restrict__ last_pos, const float* __restrict__ cmap, float cblend) {
+    float* __restrict__ T_last, int* __restrict__ last_pos, const float* __restrict__ cmap, float cblend,
+    long long idx_stride, long long cmap_stride) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND, CB>;
   __shared__ typename TW::Rec s_pi[kCtaWarps<TS>()][kChunk];
+  // a batch of candidates is one grid over all their tiles: candidate b's
+  // records, lists and images follow candidate b-1's
+  const int gt = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
+  const int b = gt / g.T, tile = gt - b * g.T;
+  const size_t pix = (size_t)b * g.H * g.W;
+  prims += (size_t)b * g.N;
+  offs += (size_t)b * (g.T + 1);
+  idx += (size_t)b * idx_stride;
+  out_color += 3 * pix; out_alpha += pix; T_last += pix; last_pos += pix;
   TW tw;
-  tw.cmap = cmap;
+  tw.cmap = CB ? cmap + (size_t)b * cmap_stride : cmap;
   tw.cblend = cblend;
-  const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
   tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float C[NP][3], T[NP], Tl[NP];
   int lp[NP];
@@ -947,14 +956,22 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS, KIND, CB>()
     Geom g, const PrimInfo* __restrict__ prims, const void* __restrict__ atlas, const int* __restrict__ offs,
     const int* __restrict__ idx, const float* __restrict__ T_last, const int* __restrict__ last_pos,
     const float* __restrict__ grad_color, const float* __restrict__ grad_alpha, double* __restrict__ gacc,
-    const float* __restrict__ cmap, float cblend) {
+    const float* __restrict__ cmap, float cblend, long long idx_stride, long long cmap_stride) {
   constexpr int NP = DefaultNP<TS>::v;
   using TW = TileWalker<TS, NP, KIND, CB>;
   __shared__ typename TW::Rec s_pi[kCtaWarps<TS>()][kChunk];
+  const int gt = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
+  const int b = gt / g.T, tile = gt - b * g.T;     // candidate and tile (see forward_kernel)
+  const size_t pix = (size_t)b * g.H * g.W;
+  prims += (size_t)b * g.N;
+  offs += (size_t)b * (g.T + 1);
+  idx += (size_t)b * idx_stride;
+  T_last += pix; last_pos += pix; grad_color += 3 * pix;
+  if (grad_alpha != nullptr) grad_alpha += pix;
+  gacc += (size_t)b * g.N * 8;
   TW tw;
-  tw.cmap = cmap;
+  tw.cmap = CB ? cmap + (size_t)b * cmap_stride : cmap;
   tw.cblend = cblend;
-  const int tile = blockIdx.x / kParts<TS>(), part = blockIdx.x % kParts<TS>();
   tw.init(g, tile, part, kCtaWarps<TS>(), offs);
   float gC[NP][3], gA[NP], Ts[NP];
   int lp[NP];
@@ -1105,20 +1122,25 @@ __global__ void __launch_bounds__(kThreadsOf<TS>(), kBlocksPerSM<TS, KIND>()) fu
   else if ((ts) == 16) { constexpr int TSV = 16; __VA_ARGS__; }      \
   else { set_error("tile_size %d is not supported (16 or 32)", ts); return DBMP_ERR_INVALID; }
 
+// batch > 1: `batch` candidates of the same canvas in one grid, candidate b's
+// records at prims + b N, lists at offs + b (T+1) / idx + b idx_stride,
+// images at b H W (x3 for colour), colour maps at cmap + b cmap_stride.
 int launch_forward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                          const int* idx, float* color, float* alpha, float* T_last, int* last_pos, const float* cmap,
-                         float cblend, cudaStream_t st) {
-  if (g.T == 0) return DBMP_OK;
+                         float cblend, cudaStream_t st, int batch, long long idx_stride, long long cmap_stride) {
+  if (g.T == 0 || batch == 0) return DBMP_OK;
+  const long long ctas = (long long)batch * g.T * kParts<32>();
+  if (ctas > 0x7fffffffll) { set_error("forward: %d candidates x %d tiles exceed one grid", batch, g.T); return DBMP_ERR_INVALID; }
   if (cmap != nullptr && cblend > 0.f) {
     DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD, true>
-                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                 <<<batch * g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                      g, prims, atlas, offs, idx, color, alpha, T_last, last_pos,
-                                                     cmap, cblend))));
+                                                     cmap, cblend, idx_stride, cmap_stride))));
   } else {
     DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (forward_kernel<TSV, KD, false>
-                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                 <<<batch * g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                      g, prims, atlas, offs, idx, color, alpha, T_last, last_pos,
-                                                     nullptr, 0.f))));
+                                                     nullptr, 0.f, idx_stride, 0))));
   }
   DBMP_CHECK_LAUNCH("forward_kernel");
   return DBMP_OK;
@@ -1126,7 +1148,8 @@ int launch_forward_blend(const Geom& g, int kind, const PrimInfo* prims, const v
 
 int launch_forward(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                    const int* idx, float* color, float* alpha, float* T_last, int* last_pos, cudaStream_t st) {
-  return launch_forward_blend(g, kind, prims, atlas, offs, idx, color, alpha, T_last, last_pos, nullptr, 0.f, st);
+  return launch_forward_blend(g, kind, prims, atlas, offs, idx, color, alpha, T_last, last_pos, nullptr, 0.f, st, 1,
+                              0, 0);
 }
 
 int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs, const int* idx,
@@ -1140,18 +1163,21 @@ int launch_count(const Geom& g, int kind, const PrimInfo* prims, const void* atl
 
 int launch_backward_blend(const Geom& g, int kind, const PrimInfo* prims, const void* atlas, const int* offs,
                           const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
-                          const float* grad_alpha, double* gacc, const float* cmap, float cblend, cudaStream_t st) {
-  if (g.T == 0) return DBMP_OK;
+                          const float* grad_alpha, double* gacc, const float* cmap, float cblend, cudaStream_t st,
+                          int batch, long long idx_stride, long long cmap_stride) {
+  if (g.T == 0 || batch == 0) return DBMP_OK;
+  const long long ctas = (long long)batch * g.T * kParts<32>();
+  if (ctas > 0x7fffffffll) { set_error("backward: %d candidates x %d tiles exceed one grid", batch, g.T); return DBMP_ERR_INVALID; }
   if (cmap != nullptr && cblend > 0.f) {
     DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD, true>
-                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                 <<<batch * g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                      g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
-                                                     grad_alpha, gacc, cmap, cblend))));
+                                                     grad_alpha, gacc, cmap, cblend, idx_stride, cmap_stride))));
   } else {
     DBMP_TS_SWITCH(g.TS, DBMP_KIND_SWITCH(kind, (backward_kernel<TSV, KD, false>
-                                                 <<<g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
+                                                 <<<batch * g.T * kParts<TSV>(), kThreadsOf<TSV>(), 0, st>>>(
                                                      g, prims, atlas, offs, idx, T_last, last_pos, grad_color,
-                                                     grad_alpha, gacc, nullptr, 0.f))));
+                                                     grad_alpha, gacc, nullptr, 0.f, idx_stride, 0))));
   }
   DBMP_CHECK_LAUNCH("backward_kernel");
   return DBMP_OK;
@@ -1161,7 +1187,7 @@ int launch_backward(const Geom& g, int kind, const PrimInfo* prims, const void* 
                     const int* idx, const float* T_last, const int* last_pos, const float* grad_color,
                     const float* grad_alpha, double* gacc, cudaStream_t st) {
   return launch_backward_blend(g, kind, prims, atlas, offs, idx, T_last, last_pos, grad_color, grad_alpha, gacc,
-                               nullptr, 0.f, st);
+                               nullptr, 0.f, st, 1, 0, 0);
 }
 
 int launch_finalize(const Geom& g, const float* radii, const float* rot, const float* opac, const float* colors,

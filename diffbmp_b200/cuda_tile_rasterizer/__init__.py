@@ -141,11 +141,8 @@ class TileRasterizerBatchFunction(Function):
     def backward(ctx, grad_out_color, grad_out_alpha):
         means2D, radii, rotations, opacities, colors, tmpl, sel = ctx.saved_tensors
         from . import _ext
-        g = _ext._get(ctx.use_fp16)
-        B = means2D.shape[0]
-        outs = [_ext.backward(ctx.use_fp16, grad_out_color[b], None if grad_out_alpha is None else grad_out_alpha[b],
-                              radii[b], rotations[b], opacities[b], colors[b], saved=g.states[b]) for b in range(B)]
-        grads = tuple(torch.stack([o[k] for o in outs]) for k in range(5))
+        # one backward launch over every candidate (the reference loops, __init__.py:195-252)
+        grads = _ext.backward_batch(ctx.use_fp16, grad_out_color, grad_out_alpha, radii, rotations, opacities, colors)
         return (*grads, None, None, None, None, None, None, None, None, None, None, None)
 
 

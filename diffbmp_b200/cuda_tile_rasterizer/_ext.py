@@ -29,6 +29,7 @@ class _Global:
         self.atlas_key = None
         self.atlas = None
         self.states = []
+        self.batch_state = None     # (BatchState, rasterizer, atlas) of the last forward_batch
         self.t_fwd = self.t_bwd = 0.0
         self.n_fwd = self.n_bwd = 0
 
@@ -100,6 +101,59 @@ def backward(fp16, grad_color, grad_alpha, radii, rotations, opacities, colors, 
     g.t_bwd += (time.perf_counter() - t0) * 1e3
     g.n_bwd += 1
     out = (gm, gr, gth, gv, gc)
+    if fp16:
+        out = tuple(x.half() for x in out)
+    return out
+
+
+def forward_batch(fp16, means2D, radii, rotations, opacities, colors, colors_orig, templates, sel, c_blend,
+                  mappings):
+    """B candidates (leading dimension) in one forward launch.  mappings: a
+    list of B reference mapping tensors, one tensor shared by every candidate
+    (the FP16 extension's form, tile_rasterize_fp16.cpp:501-560), or None
+    (device binning per candidate).  Keeps the batch state for backward_batch
+    and returns (color (B,H,W,3), alpha (B,H,W))."""
+    g = _get(fp16)
+    t0 = time.perf_counter()
+    atlas = g.get_atlas(templates)
+    B = int(radii.shape[0])
+    m = _f(means2D).view(B, -1, 2)
+    r, th, v = _f(radii).view(B, -1), _f(rotations).view(B, -1), _f(opacities).view(B, -1)
+    c = _f(colors).view(B, -1, 3)
+    s = sel.to(torch.int32).contiguous()
+    if isinstance(mappings, torch.Tensor):
+        mappings = [mappings] * B if mappings.numel() > 0 else None
+    elif mappings is not None:
+        mappings = [mp for mp in mappings if mp is not None and mp.numel() > 0] or None
+    rz = g.rz_map if mappings is not None else g.rz_cull
+    blend = colors_orig is not None and isinstance(colors_orig, torch.Tensor) and colors_orig.numel() > 0 \
+        and float(c_blend) > 0.0
+    color, alpha, state = rz.forward_batch(m, r, th, v, c, s, atlas, mappings, None,
+                                           _f(colors_orig) if blend else None, float(c_blend) if blend else 0.0)
+    g.batch_state = (state, rz, atlas)
+    g.t_fwd += (time.perf_counter() - t0) * 1e3
+    g.n_fwd += 1
+    if fp16:
+        return color.half(), alpha.half()
+    return color, alpha
+
+
+def backward_batch(fp16, grad_color, grad_alpha, radii, rotations, opacities, colors):
+    """The five gradients of every candidate of the last forward_batch, one
+    backward launch: (B,N,2), (B,N), (B,N), (B,N), (B,N,3)."""
+    g = _get(fp16)
+    if getattr(g, "batch_state", None) is None:
+        raise RuntimeError("backward_batch must follow a forward_batch")
+    state, rz, atlas = g.batch_state
+    B = int(radii.shape[0])
+    if state.batch != B:
+        raise RuntimeError(f"backward_batch of {B} candidates after a forward_batch of {state.batch}")
+    t0 = time.perf_counter()
+    out = rz.backward_batch(state, _f(grad_color), None if grad_alpha is None else _f(grad_alpha),
+                            _f(radii).view(B, -1), _f(rotations).view(B, -1), _f(opacities).view(B, -1),
+                            _f(colors).view(B, -1, 3), atlas)
+    g.t_bwd += (time.perf_counter() - t0) * 1e3
+    g.n_bwd += 1
     if fp16:
         out = tuple(x.half() for x in out)
     return out

@@ -26,33 +26,18 @@ def rasterize_tiles_backward_class(grad_out_color, grad_out_alpha, means2D, radi
 
 def rasterize_tiles_batch_class(means2D, radii, rotations, opacities, colors, colors_orig, primitive_templates,
                                 global_bmp_sel, c_blend, tile_primitive_mappings):
-    """(B,N,...) batch; one forward per candidate like tile_rasterize.cu:500-568,
-    but every candidate keeps its own state, so the batch backward is exact
-    for every candidate (the reference reuses the last candidate's caches)."""
-    import torch
-    B = means2D.shape[0]
-    maps = tile_primitive_mappings if tile_primitive_mappings is not None else []
-    cols, alps, states = [], [], []
-    for b in range(B):
-        mp = maps[b] if b < len(maps) else None
-        co = colors_orig[b] if colors_orig is not None and colors_orig.dim() == 5 else colors_orig
-        c, a, st = _ext.forward(FP16, means2D[b], radii[b], rotations[b], opacities[b], colors[b], co,
-                                primitive_templates, global_bmp_sel, c_blend, mp, keep=False)
-        cols.append(c); alps.append(a); states.append(st)
-    _ext._get(FP16).states = states
-    return torch.stack(cols), torch.stack(alps)
+    """(B,N,...) batch (tile_rasterize.cu:500-568): one forward launch over
+    every candidate's tiles.  Every candidate keeps its own state, so the
+    batch backward is exact for every candidate (the reference reuses the last
+    candidate's caches)."""
+    return _ext.forward_batch(FP16, means2D, radii, rotations, opacities, colors, colors_orig, primitive_templates,
+                              global_bmp_sel, c_blend, tile_primitive_mappings)
 
 
 def rasterize_tiles_backward_batch_class(grad_out_color, grad_out_alpha, means2D, radii, rotations, opacities, colors,
                                          colors_orig, primitive_templates, global_bmp_sel, c_blend, lr_config):
-    import torch
-    g = _ext._get(FP16)
-    B = means2D.shape[0]
-    if len(g.states) != B:
-        raise RuntimeError("backward_batch must follow a forward_batch of the same size")
-    outs = [_ext.backward(FP16, grad_out_color[b], None if grad_out_alpha is None else grad_out_alpha[b], radii[b],
-                          rotations[b], opacities[b], colors[b], saved=g.states[b]) for b in range(B)]
-    return tuple(torch.stack([o[k] for o in outs]) for k in range(5))
+    """Batch backward (tile_rasterize.cu:571-636): one launch."""
+    return _ext.backward_batch(FP16, grad_out_color, grad_out_alpha, radii, rotations, opacities, colors)
 
 
 def print_cuda_timing_stats():

@@ -3,8 +3,6 @@
 in half, transmittance included; here the atlas is stored in half and the
 arithmetic, transmittance and gradient sums stay in FP32 (an improved-accuracy
 superset).  Inputs and outputs are float16 tensors as in the reference."""
-import torch
-
 from .. import _ext
 
 FP16 = True
@@ -29,16 +27,10 @@ def rasterize_tiles_backward_class_fp16(grad_out_color, grad_out_alpha, means2D,
 
 def rasterize_tiles_batch_class_fp16(means2D, radii, rotations, opacities, colors, colors_orig, primitive_templates,
                                      global_bmp_sel, c_blend, tile_primitive_mapping):
-    """One shared mapping for the whole batch (ext_fp16.cpp:53-70)."""
-    B = means2D.shape[0]
-    cols, alps, states = [], [], []
-    for b in range(B):
-        co = colors_orig[b] if colors_orig is not None and colors_orig.dim() == 5 else colors_orig
-        c, a = _ext.forward(FP16, means2D[b], radii[b], rotations[b], opacities[b], colors[b], co,
-                            primitive_templates, global_bmp_sel, c_blend, tile_primitive_mapping)
-        cols.append(c); alps.append(a); states.append(_ext._get(FP16).states[-1])
-    _ext._get(FP16).states = states
-    return torch.stack(cols), torch.stack(alps)
+    """One mapping shared by the whole batch (ext_fp16.cpp:53-70); one
+    forward launch over every candidate's tiles."""
+    return _ext.forward_batch(FP16, means2D, radii, rotations, opacities, colors, colors_orig, primitive_templates,
+                              global_bmp_sel, c_blend, tile_primitive_mapping)
 
 
 def print_cuda_timing_stats_fp16():

@@ -111,6 +111,25 @@ class TileLists:
 
 
 @dataclass
+class BatchState:
+    """Forward state of a batch of candidates (Rasterizer.forward_batch):
+    records (B*N,16), lists offsets (B,T+1) / indices (B,stride), per-pixel
+    T_last / last_pos (B,H,W), the colour maps of a blended render."""
+    prim_info: torch.Tensor
+    offsets: torch.Tensor
+    indices: torch.Tensor
+    T_last: torch.Tensor
+    last_pos: torch.Tensor
+    colors_orig: Optional[torch.Tensor] = None
+    cmap_stride: int = 0
+    c_blend: float = 0.0
+
+    @property
+    def batch(self) -> int:
+        return int(self.offsets.shape[0])
+
+
+@dataclass
 class ForwardState:
     prim_info: torch.Tensor
     lists: TileLists
@@ -239,6 +258,103 @@ class Rasterizer:
              _ptr(last_pos), _stream(stream))
         return color, alpha, ForwardState(prim_info, lists, T_last, last_pos, cmap, float(c_blend))
 
+    # -- batches of candidates -------------------------------------------------
+    def bin_batch(self, means2D, radii, rotations, opacities, colors, sel, atlas: Atlas, stream=None):
+        """Device binning of B candidates (leading dimension of every parameter
+        tensor; sel (N) shared or (B,N)) into slots of shared buffers: records
+        (B*N,16), offsets (B,T+1), indices (B,capacity).  One host
+        synchronisation reads the B list lengths."""
+        B, N = int(radii.shape[0]), int(radii.shape[1])
+        cv = self.canvas(N, atlas)
+        st = _stream(stream)
+        prim = torch.empty((max(B * N, 1), 16), dtype=torch.float32, device=self.device)
+        offsets = torch.empty((B, self.T + 1), dtype=torch.int32, device=self.device)
+        small = torch.zeros((B, 2), dtype=torch.int32, device=self.device)    # per candidate: L, overflow
+        sel2 = sel if sel.dim() == 2 else sel.unsqueeze(0).expand(B, -1)
+        for _ in range(3):
+            self._ensure(cv, self.capacity)
+            ws, wsb = self._ws_ptr()
+            cap = max(self.capacity, 1)
+            indices = torch.empty((B, cap), dtype=torch.int32, device=self.device)
+            for b in range(B):
+                call("dbmp_bin", ctypes.byref(cv), _ptr(means2D[b]), _ptr(radii[b]), _ptr(rotations[b]),
+                     _ptr(opacities[b]), _ptr(colors[b]), _ptr(sel2[b]), _ptr(atlas.bbox),
+                     ctypes.c_void_p(prim.data_ptr() + b * N * 64), _ptr(offsets[b]), _ptr(indices[b]),
+                     ctypes.c_longlong(self.capacity), _ptr(small[b]), ctypes.c_void_p(small[b].data_ptr() + 4),
+                     ws, ctypes.c_size_t(wsb), st)
+            Ls = small.cpu()
+            if not bool(Ls[:, 1].any()):
+                return prim, offsets, indices
+            self._ensure(cv, int(int(Ls[:, 0].max()) * 1.25) + 4096)
+        raise DbmpError("binning capacity did not converge")
+
+    def forward_batch(self, means2D, radii, rotations, opacities, colors, sel, atlas: Atlas, mappings=None,
+                      stream=None, colors_orig: Optional[torch.Tensor] = None, c_blend: float = 0.0):
+        """B candidates of this canvas in one launch.  means2D (B,N,2), radii /
+        rotations / opacities (B,N), colors (B,N,3), sel (N) or (B,N);
+        mappings: None (device binning) or B reference mapping tensors;
+        colors_orig (N,Ht,Wt,3) shared or (B,N,Ht,Wt,3).  Returns
+        (color (B,H,W,3), alpha (B,H,W), BatchState)."""
+        _need_cuda(means2D, radii, rotations, opacities, colors, sel)
+        B, N = int(radii.shape[0]), int(radii.shape[1])
+        st = _stream(stream)
+        if mappings is not None and len(mappings) > 0:
+            if len(mappings) != B:
+                raise ValueError(f"{len(mappings)} mappings for {B} candidates")
+            lists = [lists_from_mapping(m, self.T, N) for m in mappings]
+            stride = max(max(l.length for l in lists), 1)
+            offsets = torch.stack([l.offsets for l in lists])
+            indices = torch.zeros((B, stride), dtype=torch.int32, device=self.device)
+            for b, l in enumerate(lists):
+                indices[b, :l.length] = l.indices[:l.length]
+            prim = torch.empty((max(B * N, 1), 16), dtype=torch.float32, device=self.device)
+            cv = self.canvas(N, atlas)
+            sel2 = sel if sel.dim() == 2 else sel.unsqueeze(0).expand(B, -1)
+            for b in range(B):
+                call("dbmp_prepare", ctypes.byref(cv), _ptr(means2D[b]), _ptr(radii[b]), _ptr(rotations[b]),
+                     _ptr(opacities[b]), _ptr(colors[b]), _ptr(sel2[b]),
+                     ctypes.c_void_p(prim.data_ptr() + b * N * 64), st)
+        else:
+            prim, offsets, indices = self.bin_batch(means2D, radii, rotations, opacities, colors, sel, atlas, stream)
+        cmap, cstride = None, 0
+        if colors_orig is not None and colors_orig.numel() > 0 and float(c_blend) > 0.0:
+            if colors_orig.dim() == 5:
+                cmap = self._colour_maps(colors_orig.reshape(B * N, *colors_orig.shape[2:]), c_blend, B * N, atlas)
+                cstride = N * atlas.Ht * atlas.Wt * 3
+            else:
+                cmap = self._colour_maps(colors_orig, c_blend, N, atlas)
+        cv = self.canvas(N, atlas)
+        dev = self.device
+        color = torch.empty((B, self.H, self.W, 3), dtype=torch.float32, device=dev)
+        alpha = torch.empty((B, self.H, self.W), dtype=torch.float32, device=dev)
+        T_last = torch.empty((B, self.H, self.W), dtype=torch.float32, device=dev)
+        last_pos = torch.empty((B, self.H, self.W), dtype=torch.int32, device=dev)
+        call("dbmp_forward_batch", ctypes.byref(cv), B, _ptr(prim), _ptr(atlas.data), _ptr(offsets), _ptr(indices),
+             ctypes.c_longlong(indices.shape[1]), _ptr(cmap), ctypes.c_longlong(cstride),
+             ctypes.c_float(c_blend if cmap is not None else 0.0), _ptr(color), _ptr(alpha), _ptr(T_last),
+             _ptr(last_pos), st)
+        return color, alpha, BatchState(prim, offsets, indices, T_last, last_pos, cmap, cstride,
+                                        float(c_blend) if cmap is not None else 0.0)
+
+    def backward_batch(self, state: BatchState, grad_color, grad_alpha, radii, rotations, opacities, colors,
+                       atlas: Atlas, stream=None):
+        """The five gradients of each candidate, in one launch: (B,N,2),
+        (B,N), (B,N), (B,N), (B,N,3)."""
+        B, N = int(radii.shape[0]), int(radii.shape[1])
+        cv = self.canvas(N, atlas)
+        dev = self.device
+        gc = _f32(grad_color)
+        ga = _f32(grad_alpha) if grad_alpha is not None else None
+        acc = torch.empty((max(B * N, 1), 8), dtype=torch.float64, device=dev)
+        outs = [torch.empty(sh, dtype=torch.float32, device=dev)
+                for sh in ((B, N, 2), (B, N), (B, N), (B, N), (B, N, 3))]
+        call("dbmp_backward_batch", ctypes.byref(cv), B, _ptr(state.prim_info), _ptr(atlas.data),
+             _ptr(state.offsets), _ptr(state.indices), ctypes.c_longlong(state.indices.shape[1]),
+             _ptr(state.colors_orig), ctypes.c_longlong(state.cmap_stride), ctypes.c_float(state.c_blend),
+             _ptr(state.T_last), _ptr(state.last_pos), _ptr(gc), _ptr(ga), _ptr(radii), _ptr(rotations),
+             _ptr(opacities), _ptr(colors), _ptr(acc), *[_ptr(o) for o in outs], _stream(stream))
+        return tuple(outs)
+
     @staticmethod
     def _colour_maps(colors_orig, c_blend, N, atlas: Atlas):
         """The (N,Ht,Wt,3) f32 colour maps of a blended render, or None."""
@@ -320,6 +436,52 @@ class RasterizeFunction(torch.autograd.Function):
         sh = ctx.shapes
         return (gm.view(sh[0]), gr.view(sh[1]), gth.view(sh[2]), gv.view(sh[3]), gc.view(sh[4]),
                 None, None, None, None, None, None)
+
+
+class RasterizeBatchFunction(torch.autograd.Function):
+    """Differentiable render of B candidates in one launch per direction.
+
+    forward(means2D (B,N,2), radii (B,N), rotations (B,N), opacities (B,N),
+            colors (B,N,3), sel (N) or (B,N), atlas, rasterizer, mappings,
+            colors_orig, c_blend) -> (color (B,H,W,3), alpha (B,H,W))
+    Gradients flow to the five parameter tensors of every candidate, as in the
+    reference's TileRasterizerBatchFunction (cuda_tile_rasterizer/__init__.py:
+    124-252), whose backward loops over the candidates.
+    """
+
+    @staticmethod
+    def forward(ctx, means2D, radii, rotations, opacities, colors, sel, atlas, rasterizer, mappings=None,
+                colors_orig=None, c_blend=0.0):
+        B = int(radii.shape[0])
+        m, r, th, v, c = (_f32(t) for t in (means2D, radii, rotations, opacities, colors))
+        s = sel.detach().to(torch.int32).contiguous()
+        color, alpha, state = rasterizer.forward_batch(m.view(B, -1, 2), r.view(B, -1), th.view(B, -1),
+                                                       v.view(B, -1), c.view(B, -1, 3), s, atlas, mappings, None,
+                                                       None if colors_orig is None else colors_orig.detach(),
+                                                       float(c_blend))
+        ctx.state, ctx.atlas, ctx.rasterizer = state, atlas, rasterizer
+        ctx.shapes = (means2D.shape, radii.shape, rotations.shape, opacities.shape, colors.shape)
+        ctx.save_for_backward(r, th, v, c)
+        return color, alpha
+
+    @staticmethod
+    def backward(ctx, grad_color, grad_alpha):
+        r, th, v, c = ctx.saved_tensors
+        rz: Rasterizer = ctx.rasterizer
+        B = int(ctx.state.batch)
+        if grad_color is None:
+            grad_color = torch.zeros((B, rz.H, rz.W, 3), dtype=torch.float32, device=r.device)
+        g = rz.backward_batch(ctx.state, grad_color, grad_alpha, r.view(B, -1), th.view(B, -1), v.view(B, -1),
+                              c.view(B, -1, 3), ctx.atlas)
+        sh = ctx.shapes
+        return (g[0].view(sh[0]), g[1].view(sh[1]), g[2].view(sh[2]), g[3].view(sh[3]), g[4].view(sh[4]),
+                None, None, None, None, None, None)
+
+
+def rasterize_batch(means2D, radii, rotations, opacities, colors, sel, atlas: Atlas, rasterizer: Rasterizer,
+                    mappings=None, colors_orig: Optional[torch.Tensor] = None, c_blend: float = 0.0):
+    return RasterizeBatchFunction.apply(means2D, radii, rotations, opacities, colors, sel, atlas, rasterizer,
+                                        mappings, colors_orig, c_blend)
 
 
 def rasterize(means2D, radii, rotations, opacities, colors, sel, atlas: Atlas, rasterizer: Rasterizer,

@@ -111,22 +111,26 @@ class Server:
         self.keep_params = keep_params
 
     def _reserve(self, requests: List[JobRequest]):
-        """Grows the device allocator's cache to the jobs' estimated total
-        (within the HBM budget) before serving: job set-up then carves its
+        """Grows the device allocator's cache to the resident jobs' estimated
+        total (within the HBM budget) before serving: job set-up then carves its
         buffers from cached memory instead of allocating device memory while
         the device is busy, which stalled the host for up to 0.2 s.  The
         allocator reuses a cached block only on the stream it was allocated
         on, so the blocks are allocated on the admission stream: one large
         block for the large pool, and 1 MB blocks for the small pool's
         segments (tensors of up to 1 MB: counters, offsets, small jobs' state)."""
-        want = min(self.budget, float(sum(estimate_bytes(r.spec, self.cfg.tile_size) for r in requests)))
+        # at most max_slots jobs are resident at once: the largest max_slots estimates bound them
+        est = sorted(estimate_bytes(r.spec, self.cfg.tile_size) for r in requests)[-self.max_slots:]
+        want = min(self.budget, float(sum(est)))
         free, _ = torch.cuda.mem_get_info()
         want = int(min(want, 0.8 * free))
         with torch.cuda.stream(self.admit_stream):
             if want > (1 << 26):
                 block = torch.empty(want, dtype=torch.uint8, device="cuda")
                 del block
-            small = [torch.empty(1 << 20, dtype=torch.uint8, device="cuda") for _ in range(16 * len(requests))]
+            # segments for the jobs that can be resident at once, not for the whole stream
+            small = [torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
+                     for _ in range(16 * min(len(requests), self.max_slots))]
             del small
 
     def _admit(self, req: JobRequest, now: float, stream) -> _Slot:
@@ -267,7 +271,10 @@ def summarize(results: List[JobResult]):
 
 
 def run_sequential(requests: List[JobRequest], atlas_templates, kind="f32", fused=False, lr=0.01, graphs=False):
-    """One job at a time, to completion: the plain baseline of the serving target."""
+    """One job at a time, to completion: the baselines of the serving target.
+    Each job is set up as the server sets one up (lists sized from
+    list_capacity_bound, the iteration captured in a CUDA graph when
+    `graphs`), then runs its iterations and reads its result."""
     atlas = Atlas(atlas_templates, kind)
     cfg = FitConfig(lr=lr, fused=fused)
     out = []
@@ -275,7 +282,7 @@ def run_sequential(requests: List[JobRequest], atlas_templates, kind="f32", fuse
     for req in requests:
         s = req.spec
         f = ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, atlas, s.target,
-                        s.background, cfg)
+                        s.background, cfg, list_capacity=list_capacity_bound(s, cfg.tile_size))
         if graphs:
             f.capture()
         for _ in range(req.iterations):

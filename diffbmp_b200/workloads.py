@@ -185,6 +185,19 @@ def smooth_field_device(rng: np.random.Generator, H: int, W: int, device, n: int
     return out.contiguous()
 
 
+_WHITE = {}
+
+
+def white_background(H: int, W: int, device):
+    """A white (H,W,3) background on `device`, one read-only tensor per size
+    shared by every job of that size."""
+    import torch
+    key = (H, W, str(device))
+    if key not in _WHITE:
+        _WHITE[key] = torch.ones((H, W, 3), dtype=torch.float32, device=device)
+    return _WHITE[key]
+
+
 def make_job(rng: np.random.Generator, atlas: np.ndarray, sizes=(256, 512, 1024, 2048),
              n_range=(256, 20000), device=None) -> SceneSpec:
     """One serving job: W and H drawn independently from `sizes`, N log-uniform
@@ -195,9 +208,8 @@ def make_job(rng: np.random.Generator, atlas: np.ndarray, sizes=(256, 512, 1024,
     P = atlas.shape[0]
     means2D, r, th, v, c, sel = sample_params(rng, H, W, N, P, "uniform")
     if device is not None:
-        import torch
         target = smooth_field_device(rng, H, W, device, noise=0.02)
-        bg = torch.ones((H, W, 3), dtype=torch.float32, device=device)
+        bg = white_background(H, W, device)
     else:
         target = smooth_field(rng, H, W, noise=0.02)
         bg = np.ones((H, W, 3), np.float32)

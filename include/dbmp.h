@@ -232,6 +232,31 @@ int dbmp_backward_blend(const dbmp_canvas* cv, const void* prim_info, const void
                         float* grad_radii, float* grad_rotations, float* grad_opacities,
                         float* grad_colors, void* stream);
 
+/* Forward / backward of a batch of `batch` candidates of the same canvas,
+ * atlas and template assignment in one launch: one grid over every
+ * candidate's tiles, so a batch of small canvases fills the GPU.  Candidate b
+ * has its records at prim_info + b*N (prepared per candidate, e.g. by dbmp_bin
+ * into that slot), its lists at tile_offsets + b*(T+1) and tile_indices +
+ * b*index_stride, its images at b*H*W (x3 for colour), its parameters at b*N
+ * (x2 for means2D, x3 for colors), its gradient sums at grad_accum + b*N*8
+ * and its colour maps at colors_orig + b*colors_orig_stride (stride 0: shared
+ * maps).  Otherwise as dbmp_forward_blend / dbmp_backward_blend for each
+ * candidate.  Replaces TileRasterizer::forward_batch / backward_batch
+ * (cuda_tile_rasterizer/tile_rasterize.cu:500-636), which loop over the
+ * candidates on the host. */
+int dbmp_forward_batch(const dbmp_canvas* cv, int batch, const void* prim_info, const void* atlas,
+                       const int32_t* tile_offsets, const int32_t* tile_indices, long long index_stride,
+                       const float* colors_orig, long long colors_orig_stride, float c_blend, float* out_color,
+                       float* out_alpha, float* T_last, int32_t* last_pos, void* stream);
+int dbmp_backward_batch(const dbmp_canvas* cv, int batch, const void* prim_info, const void* atlas,
+                        const int32_t* tile_offsets, const int32_t* tile_indices, long long index_stride,
+                        const float* colors_orig, long long colors_orig_stride, float c_blend,
+                        const float* T_last, const int32_t* last_pos, const float* grad_color,
+                        const float* grad_alpha, const float* radii, const float* rotations,
+                        const float* opacities, const float* colors, double* grad_accum,
+                        float* grad_means2D, float* grad_radii, float* grad_rotations,
+                        float* grad_opacities, float* grad_colors, void* stream);
+
 /* Counting pass over the same walk as dbmp_forward (no image output):
  * counts[0] = (pixel, primitive) pairs that pass the square cull before the
  * pixel terminates, counts[1] = fragments composited, counts[2] = tile-list

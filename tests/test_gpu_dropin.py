@@ -89,35 +89,57 @@ def test_bad_mapping_is_rejected():
                                      cuda(s.colors), None, cuda(s.templates), cuda(sel, torch.int32), 0.0, bad)
 
 
-def test_fp16_extension_tracks_fp32():
+def test_fp16_extension_vs_oracle():
+    """The FP16 extension (_C_fp16) quantises its inputs to half, as the
+    reference's does; on those half-rounded inputs its image is within half
+    storage and output rounding of the FP64 oracle (PSNR >= 60 dB), and its
+    gradients within 1e-2 per block."""
     import diffbmp_b200.cuda_tile_rasterizer as ctr
     s, sel = scene(3)
+    h = lambda a: np.asarray(a, np.float32).astype(np.float16).astype(np.float64)
+    sc = O.Scene(s.H, s.W, 16, h(s.means2D), h(s.radii), h(s.rotations), h(s.opacities), h(s.colors), h(s.templates),
+                 sel)
+    offs, idx = bin_scene(sc, O.BIN_CULL)
     t16 = ctr.TileRasterizer(s.H, s.W, 16, 0.0, 1.0, 400, s.N, use_fp16=True)
-    t32 = ctr.TileRasterizer(s.H, s.W, 16, 0.0, 1.0, 400, s.N, use_fp16=False)
-    args = [cuda(s.means2D), cuda(s.radii), cuda(s.rotations), cuda(s.opacities), cuda(s.colors), None,
-            cuda(s.templates), cuda(sel, torch.int32), 0.0, None, None]
-    c16, a16 = t16(*args)
-    c32, a32 = t32(*args)
+    ps = [cuda(a).half().requires_grad_() for a in (s.means2D, s.radii, s.rotations, s.opacities, s.colors)]
+    c16, a16 = t16(*ps, None, cuda(s.templates), cuda(sel, torch.int32), 0.0, None, None)
     assert c16.dtype == torch.float16
-    # positions are quantised to half by the FP16 API (as in the reference), so compare loosely
-    assert (c16.float() - c32).abs().mean().item() < 5e-3
+    ref = O.forward(sc, offs, idx)
+    err = c16.float().detach().cpu().numpy() - ref["color"]
+    psnr = 10 * np.log10(1.0 / float(np.mean(err ** 2)))
+    print("fp16 extension PSNR", psnr, "max", np.abs(err).max())
+    assert psnr >= 60.0
+    rng = np.random.default_rng(1)
+    wc = rng.normal(0, 1, (s.H, s.W, 3)).astype(np.float32)
+    (c16.float() * cuda(wc)).sum().backward()
+    g = O.backward(sc, offs, idx, wc, None)
+    ours = np.concatenate([p.grad.float().cpu().numpy().reshape(s.N, -1) for p in ps], 1)
+    for k in range(8):
+        assert np.linalg.norm(ours[:, k] - g[:, k]) <= 1e-2 * np.linalg.norm(g[:, k]), k
 
 
 def test_batch_api_gradients_are_per_candidate():
+    """forward_batch / its backward (one launch each over every candidate's
+    tiles): each candidate's image and all eight gradient blocks against the
+    FP64 oracle at the single-render bars (1e-5 image, 1e-4 gradients per
+    block, boundary band held to its spread)."""
     import diffbmp_b200.cuda_tile_rasterizer as ctr
     s, sel = scene(4, H=96, W=128, N=120)
     B = 3
     rng = np.random.default_rng(5)
     m = np.stack([s.means2D + rng.normal(0, 3, s.means2D.shape).astype(np.float32) for _ in range(B)])
+    op = np.stack([s.opacities + rng.normal(0, 0.5, s.N).astype(np.float32) for _ in range(B)])
     tr = ctr.TileRasterizer(s.H, s.W, 32, 0.0, 1.0, 400, s.N)
     params = [cuda(m).requires_grad_(), cuda(np.stack([s.radii] * B)).requires_grad_(),
-              cuda(np.stack([s.rotations] * B)).requires_grad_(), cuda(np.stack([s.opacities] * B)).requires_grad_(),
+              cuda(np.stack([s.rotations] * B)).requires_grad_(), cuda(op).requires_grad_(),
               cuda(np.stack([s.colors] * B)).requires_grad_()]
     color, alpha = tr.forward_batch(*params, None, cuda(s.templates), cuda(sel, torch.int32), 0.0, None, None)
-    color.sum().backward()
+    wc = rng.normal(0, 1, (B, s.H, s.W, 3)).astype(np.float32)
+    wa = rng.normal(0, 1, (B, s.H, s.W)).astype(np.float32)
+    ((color * cuda(wc)).sum() + (alpha * cuda(wa)).sum()).backward()
     for b in range(B):
-        sc = O.Scene(s.H, s.W, 32, m[b], s.radii, s.rotations, s.opacities, s.colors, s.templates, sel)
+        sc = O.Scene(s.H, s.W, 32, m[b], s.radii, s.rotations, op[b], s.colors, s.templates, sel)
         offs, idx = bin_scene(sc, O.BIN_CULL)
-        g = O.backward(sc, offs, idx, np.ones((s.H, s.W, 3), np.float32), None)
-        gm = params[0].grad[b].cpu().numpy()
-        assert np.linalg.norm(gm - g[:, 0:2]) <= 2e-3 * np.linalg.norm(g[:, 0:2])
+        O.check_image(sc, offs, idx, color[b].detach().cpu().numpy(), alpha[b].detach().cpu().numpy(), tol=1e-5)
+        ours = np.concatenate([p.grad[b].cpu().numpy().reshape(s.N, -1) for p in params], 1)
+        O.check_grads(sc, offs, idx, wc[b], wa[b], ours, rel=1e-4)
