@@ -62,8 +62,10 @@ def parse():
     ap.add_argument("--serving-jobs", type=int, default=2000,
                     help="jobs of the serving stream measured beside the headline (0: skip)")
     ap.add_argument("--no-psd", action="store_true", help="skip the PSD export section")
-    ap.add_argument("--profile", default=None, choices=["f16", "f32", "bf16", "f32q", "f16q", "bf16q", "plain"],
-                    help="profiling mode: one job of this form, --warmup + --steps eager steps, no timing line")
+    ap.add_argument("--profile", default=None,
+                    choices=["f16", "f32", "bf16", "f32q", "f16q", "bf16q", "plain", "psd"],
+                    help="profiling mode: one job of this form, --warmup + --steps eager steps, no timing line "
+                         "(psd: one PSD export of the 1024^2 / N=5000 case: crop kernel, count and write passes)")
     return ap.parse_args()
 
 
@@ -429,6 +431,33 @@ def run_serving(n_jobs, seed, torch, subsample=5, load=0.8):
                     "iterations ahead of the host"}
 
 
+def psd_case(torch, W, N, P_, S, seed=0):
+    """Inputs of the PSD export case: W x W canvas, N primitives, P_ templates
+    of S^2 texels, radii s*W/2 with s log-uniform in [0.05, 0.3]."""
+    from diffbmp_b200 import workloads as wl
+    rng = np.random.default_rng(seed)
+    tm = torch.from_numpy(np.stack([wl.random_shape(rng, S) for _ in range(P_)])).cuda()
+    t = lambda a: torch.from_numpy(np.asarray(a, np.float32)).cuda()
+    m = t(np.stack([rng.uniform(0, W, N), rng.uniform(0, W, N)], 1))
+    r = t(np.exp(rng.uniform(np.log(0.05), np.log(0.3), N)) * W / 2)
+    th = t(rng.uniform(0, 2 * np.pi, N))
+    vs = torch.sigmoid(t(rng.normal(0, 1, N)))
+    cs = torch.sigmoid(t(rng.normal(0, 2, (N, 3))))
+    sel = torch.from_numpy(((N - 1 - np.arange(N)) % P_).astype(np.int32)).cuda()
+    return tm, m, r, th, vs, cs, sel
+
+
+def psd_export_once(torch, W, N, P_, S):
+    """One device export of the case: crops, then the layers' PackBits channel blocks."""
+    import diffbmp_b200.psd as P
+    tm, m, r, th, vs, cs, sel = psd_case(torch, W, N, P_, S)
+    buf, bbox, sizes, offs = P.export_layers(tm, m, r, th, vs, cs, sel, W, W)
+    blob, blocks, chosen = P.encode_channel_blocks(buf, sizes, offs, sizes.cpu().numpy(), P.ORDER_LAYER,
+                                                   lambda flags: np.nonzero(flags)[0])
+    torch.cuda.synchronize()
+    return {"crop_bytes": int(buf.numel()), "encoded_bytes": int(blob.numel()), "layers": int(len(chosen))}
+
+
 def run_psd(torch, peaks):
     """PSD layer export on the device at 1024^2 / N=5000 and 2048^2 / N=20000
     (templates of the scene configs, radii s*W/2 with s log-uniform in
@@ -437,7 +466,6 @@ def run_psd(torch, peaks):
     passes of the file's channel data (dbmp_psd_rle_count / _write) -- with
     its algorithmic bytes and the fraction of the measured HBM copy peak."""
     import diffbmp_b200.psd as P
-    from diffbmp_b200 import workloads as wl
     hbm = peaks.get("hbm_gbs")
     times = {}
     real_call = P.call
@@ -456,19 +484,11 @@ def run_psd(torch, peaks):
     P.call = timed_call
     try:
         for cfg, (W, N, P_, S) in (("c1", (1024, 5000, 8, 128)), ("c2", (2048, 20000, 16, 256))):
-            rng = np.random.default_rng(0)
-            tm = torch.from_numpy(np.stack([wl.random_shape(rng, S) for _ in range(P_)])).cuda()
-            x = torch.from_numpy(rng.uniform(0, W, N).astype(np.float32)).cuda()
-            y = torch.from_numpy(rng.uniform(0, W, N).astype(np.float32)).cuda()
-            r = torch.from_numpy((np.exp(rng.uniform(np.log(0.05), np.log(0.3), N)) * W / 2).astype(np.float32)).cuda()
-            th = torch.from_numpy(rng.uniform(0, 2 * np.pi, N).astype(np.float32)).cuda()
-            vs = torch.sigmoid(torch.from_numpy(rng.normal(0, 1, N).astype(np.float32)).cuda())
-            cs = torch.sigmoid(torch.from_numpy(rng.normal(0, 2, (N, 3)).astype(np.float32)).cuda())
-            sel = torch.from_numpy(((N - 1 - np.arange(N)) % P_).astype(np.int32)).cuda()
+            tm, m, r, th, vs, cs, sel = psd_case(torch, W, N, P_, S)
             best = {}
             for _ in range(3):          # the first pass warms up; the best of the other two counts
                 times.clear()
-                buf, bbox, sizes, offs = P.export_layers(tm, torch.stack([x, y], 1), r, th, vs, cs, sel, W, W)
+                buf, bbox, sizes, offs = P.export_layers(tm, m, r, th, vs, cs, sel, W, W)
                 hs = sizes.cpu().numpy()
                 blob, blocks, chosen = P.encode_channel_blocks(buf, sizes, offs, hs, P.ORDER_LAYER,
                                                                lambda flags: np.nonzero(flags)[0])
@@ -591,6 +611,9 @@ def main():
     rank, world, local = dist_setup(args)
     from diffbmp_b200 import workloads as wl
     spec = wl.make_scene(args.config, seed=rank)
+    if args.profile == "psd":
+        print(json.dumps({"profile": "psd", "export": psd_export_once(torch, 1024, 5000, 8, 128)}))
+        return
     if args.profile:
         kind = "f32" if args.profile == "plain" else args.profile
         job = build_job(spec, kind, args.profile != "plain", torch)
