@@ -178,6 +178,12 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
   pi.cr = sigmoid_precise(colors[3 * n + 0]);
   pi.cg = sigmoid_precise(colors[3 * n + 1]);
   pi.cb = sigmoid_precise(colors[3 * n + 2]);
+  if (half_record(g.kind)) {   // the precision form stores opacity and colours in FP16
+    const __half2 ar = __floats2half2_rn(pi.alpha0, pi.cr), gb = __floats2half2_rn(pi.cg, pi.cb);
+    pi.alpha0 = __uint_as_float(*reinterpret_cast<const unsigned*>(&ar));
+    pi.cr = __uint_as_float(*reinterpret_cast<const unsigned*>(&gb));
+    pi.cg = pi.cb = 0.f;
+  }
   const bool nan_geom = isnan(pi.a00) || isnan(pi.a01) || isnan(pi.a10) || isnan(pi.a11) || isnan(mx) || isnan(my);
   pi.toff = (!valid || nan_geom) ? kNoFrag : tid * template_records(g.kind, g.Ht, g.Wt);
   // clearance a warp footprint needs before the walk may skip it: the

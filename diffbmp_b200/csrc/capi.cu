@@ -87,6 +87,10 @@ int make_geom(const dbmp_canvas* cv, Geom* g, const char* who) {
   }
   if (cv->atlas_kind < DBMP_ATLAS_F32 || cv->atlas_kind > DBMP_ATLAS_BF16_PAIR) { set_error("%s: atlas_kind %d unknown", who, cv->atlas_kind); return DBMP_ERR_INVALID; }
   if (!(cv->alpha_max >= 0.f && cv->alpha_max < INFINITY)) { set_error("%s: alpha_max %g is not a finite value >= 0", who, (double)cv->alpha_max); return DBMP_ERR_INVALID; }
+  if (half_record(cv->atlas_kind) && !(cv->alpha_max <= 65504.f)) {
+    set_error("%s: alpha_max %g exceeds the FP16 range of the half / bfloat16 atlas kinds", who, (double)cv->alpha_max);
+    return DBMP_ERR_INVALID;
+  }
   if (!(cv->t_stop >= 1e-30f && cv->t_stop < 1.f)) { set_error("%s: t_stop %g outside [1e-30, 1)", who, (double)cv->t_stop); return DBMP_ERR_INVALID; }
   if ((long long)cv->height * cv->width > (1ll << 31) / 4) { set_error("%s: canvas too large", who); return DBMP_ERR_INVALID; }
   g->H = cv->height; g->W = cv->width; g->TS = cv->tile_size;

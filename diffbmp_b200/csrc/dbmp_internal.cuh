@@ -17,6 +17,9 @@ namespace dbmp {
 // cuda_tile_rasterizer/cuda_kernels/tile_forward.cu:191-192) and
 // hx = (Wt-1)/2, hy = (Ht-1)/2.  The affine coefficients fold the reference's
 // r_inv, rotation and texel scaling (tile_forward.cu:250-264).
+// With a half or bfloat16 atlas (the precision form) the opacity and colours
+// are stored in FP16 as well: the third word then holds the bit patterns of
+// the half pairs (alpha0, cr) and (cg, cb) in alpha0 and cr, and zeros.
 struct __align__(16) PrimInfo {
   float mx, my, hw, hh;      // centre, square-cull half extents (tile_forward.cu:194-210)
   float a00, a01, a10, a11;  // inverse affine to texel coordinates
@@ -79,6 +82,11 @@ __host__ __device__ inline void grid_shape(int n, int* shift, int* cells) {
 }
 
 __host__ __device__ inline bool atlas_has_grid(int kind) { return kind != ATLAS_F32; }
+
+// Atlas kinds of the precision form: texels, opacity and colours in 16 bits.
+__host__ __device__ constexpr bool half_record(int kind) {
+  return kind == ATLAS_F16_QUAD || kind == ATLAS_BF16_QUAD || kind == ATLAS_F16_PAIR || kind == ATLAS_BF16_PAIR;
+}
 
 // Bytes of the texel records of an atlas kind (a packed atlas's grid follows them).
 __host__ __device__ inline size_t atlas_record_bytes(int P, int Ht, int Wt, int kind) {

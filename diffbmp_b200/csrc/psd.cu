@@ -152,6 +152,20 @@ struct PsdArgs {
 
 // Stage 2 (psd_export_kernels.cu:61-198): persistent grid over the 16x16
 // blocks of all crops; block b belongs to the layer n with blk[n] <= b < blk[n+1].
+// Everything that depends only on the layer -- its index (a binary search
+// over blk), crop box, centre, radius, rotation with its cosine and sine,
+// opacity and colour -- is computed once per block by one thread and shared
+// through shared memory; each thread then computes one pixel with the
+// reference's per-pixel operations on the same values, so the bytes are the
+// ones a per-pixel evaluation gives.
+struct PsdLayer {
+  int4 bb;
+  float x, y, r, theta, cos_t, sin_t, vis, cr, cg, cb;
+  int n, t_idx;
+  long long off;
+  long long k;   // block index within the layer
+};
+
 __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float* __restrict__ means2D,
                                                          const float* __restrict__ radii,
                                                          const float* __restrict__ rot,
@@ -163,38 +177,54 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
                                                          const long long* __restrict__ blk,
                                                          const float* __restrict__ colors_orig,
                                                          uint8_t* __restrict__ out) {
+  __shared__ PsdLayer s_l;
   const long long nblk = blk[a.N];
   const int lx = threadIdx.x & (kPsdBlock - 1), ly = threadIdx.x / kPsdBlock;
   for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
-    int lo = 0, hi = a.N;   // largest n with blk[n] <= b
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (blk[mid] <= b) lo = mid; else hi = mid;
+    __syncthreads();   // every thread is done with the previous block's layer
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = a.N;   // largest n with blk[n] <= b
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (blk[mid] <= b) lo = mid; else hi = mid;
+      }
+      const int n = lo;
+      PsdLayer L;
+      L.n = n;
+      L.bb = reinterpret_cast<const int4*>(bbox)[n];
+      L.k = b - blk[n];
+      L.x = means2D[n * 2 + 0] * a.scale;
+      L.y = means2D[n * 2 + 1] * a.scale;
+      L.r = radii[n] * a.scale;
+      L.theta = rot[n];
+      L.cos_t = cosf(L.theta);
+      L.sin_t = sinf(L.theta);
+      L.vis = vis[n];
+      L.cr = colors[n * 3 + 0];
+      L.cg = colors[n * 3 + 1];
+      L.cb = colors[n * 3 + 2];
+      L.t_idx = sel[n];
+      L.off = layer_offsets[n];
+      s_l = L;
     }
-    const int n = lo;
-    const int4 bb = reinterpret_cast<const int4*>(bbox)[n];
-    const int bw = bb.z - bb.x, bh = bb.w - bb.y;
+    __syncthreads();
+    const PsdLayer L = s_l;
+    const int bw = L.bb.z - L.bb.x, bh = L.bb.w - L.bb.y;
     const int bx_n = (bw + kPsdBlock - 1) / kPsdBlock;
-    const long long k = b - blk[n];
-    const int lpx = (int)(k % bx_n) * kPsdBlock + lx, lpy = (int)(k / bx_n) * kPsdBlock + ly;
+    const int lpx = (int)(L.k % bx_n) * kPsdBlock + lx, lpy = (int)(L.k / bx_n) * kPsdBlock + ly;
     if (lpx >= bw || lpy >= bh) continue;
-    const int px = bb.x + lpx, py = bb.y + lpy;
-    const float x = means2D[n * 2 + 0] * a.scale;
-    const float y = means2D[n * 2 + 1] * a.scale;
-    const float r = radii[n] * a.scale;
-    const float theta = rot[n];
-    const float cos_t = cosf(theta), sin_t = sinf(theta);
-    const float tv = psd_template_value(tmpl, sel[n], a.P, a.Ht, a.Wt, px, py, x, y, r, cos_t, sin_t);
-    const float alpha_val = tv * vis[n] * a.alpha_max;
+    const int px = L.bb.x + lpx, py = L.bb.y + lpy;
+    const float tv = psd_template_value(tmpl, L.t_idx, a.P, a.Ht, a.Wt, px, py, L.x, L.y, L.r, L.cos_t, L.sin_t);
+    const float alpha_val = tv * L.vis * a.alpha_max;
     uchar4 px4 = make_uchar4(0, 0, 0, 0);
     if (!(alpha_val < 0.001f)) {
-      float rgb_r = colors[n * 3 + 0], rgb_g = colors[n * 3 + 1], rgb_b = colors[n * 3 + 2];
+      float rgb_r = L.cr, rgb_g = L.cg, rgb_b = L.cb;
       if (colors_orig != nullptr && a.c_blend > 0.0f) {
-        const float* cm = colors_orig + (size_t)n * a.Ht * a.Wt * 3;
-        const float ux = x / a.scale, uy = y / a.scale;
+        const float* cm = colors_orig + (size_t)L.n * a.Ht * a.Wt * 3;
+        const float ux = L.x / a.scale, uy = L.y / a.scale;
         const float upx = (float)px / a.scale, upy = (float)py / a.scale;
-        const float ur = r / a.scale;
-        const float3 co = psd_color_map(cm, a.Ht, a.Wt, upx - ux, upy - uy, ur, theta);
+        const float ur = L.r / a.scale;
+        const float3 co = psd_color_map(cm, a.Ht, a.Wt, upx - ux, upy - uy, ur, L.theta);
         rgb_r = (1.0f - a.c_blend) * rgb_r + a.c_blend * co.x;
         rgb_g = (1.0f - a.c_blend) * rgb_g + a.c_blend * co.y;
         rgb_b = (1.0f - a.c_blend) * rgb_b + a.c_blend * co.z;
@@ -202,7 +232,7 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
       const float mask = tv > 0.0f ? 1.0f : 0.0f;
       px4 = make_uchar4(to_u8(mask * rgb_r), to_u8(mask * rgb_g), to_u8(mask * rgb_b), to_u8(alpha_val));
     }
-    *reinterpret_cast<uchar4*>(out + layer_offsets[n] + ((long long)lpy * bw + lpx) * 4) = px4;
+    *reinterpret_cast<uchar4*>(out + L.off + ((long long)lpy * bw + lpx) * 4) = px4;
   }
 }
 

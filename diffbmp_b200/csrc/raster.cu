@@ -428,7 +428,11 @@ struct TileWalker {
                 const float ey = fmaf(fabsf(g1.z), g.fhx, fmaf(fabsf(g1.w), g.fhy, 0.05f));
                 fast = cx - ex >= 0.f && cx + ex <= g.wm1 && cy - ey >= 0.f && cy + ey <= g.hm1;
               }
-              const float4 g2 = __ldg(r + 2);
+              float4 g2 = __ldg(r + 2);
+              if (half_record(KIND)) {   // FP16 (alpha0, r) and (g, b) pairs
+                const float2 ar = h2f(__float_as_uint(g2.x)), gb = h2f(__float_as_uint(g2.y));
+                g2 = make_float4(ar.x, ar.y, gb.x, gb.y);
+              }
               w[lane][0] = g0;
               w[lane][1] = g1;
               if (kPair) {

@@ -129,7 +129,9 @@ def test_diffbmp_wrapper_render_and_batch():
     from diffbmp_b200.pydiffbmp.core.renderer.simple_tile_renderer import SimpleTileRenderer
     from diffbmp_b200.pydiffbmp.diffbmp_wrapper import DiffBMPWrapper
     s, S, bg, sel, amax = _setup(7, N=150)
-    s.radii[:] = np.clip(s.radii, 2.0, min(s.H, s.W) // 4)   # values the batch path leaves unclamped
+    # values the batch path's clamp leaves unchanged (x in [0, W-1], y in [0, H-1], r in [2, min(H,W)//4])
+    s.radii[:] = np.clip(s.radii, 2.0, min(s.H, s.W) // 4)
+    s.means2D[:] = np.clip(s.means2D - 3.0, 0.0, [s.W - 4.0, s.H - 4.0])
     w = DiffBMPWrapper("cuda").set_primitive(_cuda(S))
     w.canvas_size = (s.H, s.W)
     leaves = _leaves(s)
