@@ -162,8 +162,8 @@ struct PsdLayer {
   int4 bb;
   float x, y, r, theta, cos_t, sin_t, vis, cr, cg, cb;
   int n, t_idx;
+  int bx, by;    // the block's first pixel within the crop
   long long off;
-  long long k;   // block index within the layer
 };
 
 __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float* __restrict__ means2D,
@@ -192,7 +192,10 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
       PsdLayer L;
       L.n = n;
       L.bb = reinterpret_cast<const int4*>(bbox)[n];
-      L.k = b - blk[n];
+      const int bx_n = (L.bb.z - L.bb.x + kPsdBlock - 1) / kPsdBlock;   // blocks per crop row
+      const long long k = b - blk[n];
+      L.bx = (int)(k % bx_n) * kPsdBlock;
+      L.by = (int)(k / bx_n) * kPsdBlock;
       L.x = means2D[n * 2 + 0] * a.scale;
       L.y = means2D[n * 2 + 1] * a.scale;
       L.r = radii[n] * a.scale;
@@ -210,8 +213,7 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
     __syncthreads();
     const PsdLayer L = s_l;
     const int bw = L.bb.z - L.bb.x, bh = L.bb.w - L.bb.y;
-    const int bx_n = (bw + kPsdBlock - 1) / kPsdBlock;
-    const int lpx = (int)(L.k % bx_n) * kPsdBlock + lx, lpy = (int)(L.k / bx_n) * kPsdBlock + ly;
+    const int lpx = L.bx + lx, lpy = L.by + ly;
     if (lpx >= bw || lpy >= bh) continue;
     const int px = L.bb.x + lpx, py = L.bb.y + lpy;
     const float tv = psd_template_value(tmpl, L.t_idx, a.P, a.Ht, a.Wt, px, py, L.x, L.y, L.r, L.cos_t, L.sin_t);
@@ -243,10 +245,13 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 // then PSDImage.save; psd_export_uint8.py:153-186, psd_exporter.py:468-501),
 // which splits it into planes and RLE-compresses them row by row on the host.
 // Here every (layer, channel, row) is encoded on the device.  Rows are taken
-// 32 at a time, one warp per group of 32 rows of a layer and one lane per
-// row; each lane runs four encoders at once, one per RGBA byte, on uchar4
-// pixels that the warp stages through shared memory 32 rows x 32 pixels at a
-// time (coalesced loads, conflict-free reads with a 33-word row pitch).
+// 32 at a time: one CTA of 128 threads per group of 32 rows of a layer, one
+// thread per (row, channel slot), so each thread runs a single encoder.  The
+// CTA stages the group's uchar4 pixels through shared memory, 32 rows x 32
+// pixels at a time (coalesced loads; a 33-word row pitch keeps the reads
+// conflict-free: the four threads of a row read the same word).  In the
+// write pass each thread keeps the bytes of its row in a 256-byte ring in
+// shared memory, from which literal packets are written.
 //
 // Encoding rule (a valid PackBits stream; a packet never crosses a row):
 //   - a maximal run of L >= 3 equal bytes becomes replicate packets
@@ -254,6 +259,10 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 //     becomes the literal packet [0, v];
 //   - maximal runs of one or two bytes are gathered into literal segments,
 //     written as packets [k-1, k bytes] of 128 bytes and a last shorter one.
+// A literal segment that ends at a run of three or more is written as soon as
+// the run reaches three bytes (the packets and their order are those of
+// writing it when the run ends), so the bytes a pending literal segment needs
+// are never more than 131 behind the current one and the ring suffices.
 // The count pass writes each row's encoded size (at most w + ceil(w/128)
 // bytes, so 16 bits suffice for w <= 30000, the PSD width limit) and each
 // group's per-channel totals; the host plans where every channel block goes;
@@ -262,9 +271,11 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 // match the data can write wrong bytes but never out of bounds.
 // ---------------------------------------------------------------------------
 
-constexpr int kRleWarps = 8;      // warps per CTA
-constexpr int kRlePitch = 33;     // words per staged row (32 pixels + 1 pad)
-constexpr int kRleMaxWidth = 30000;
+constexpr int kRleRows = 32;                  // rows per group (one CTA)
+constexpr int kRleThreads = kRleRows * 4;     // one thread per (row, channel slot)
+constexpr int kRlePitch = 33;                 // words per staged row (32 pixels + 1 pad)
+constexpr int kRleRing = 256;                 // bytes of a thread's literal ring
+constexpr int kRleRingPitch = kRleRing + 4;   // ring stride: threads of a warp hit distinct banks
 
 struct RleArgs {
   const uint8_t* layers;        // packed RGBA crops, row-major per layer
@@ -284,174 +295,160 @@ struct RleArgs {
   long long out_bytes;
 };
 
-// Four PackBits encoders of one row.  COUNT only adds sizes; WRITE stores.
+// PackBits encoder of one channel row.  COUNT (WRITE false) only adds sizes;
+// WRITE stores, reading literal bytes from the thread's ring (ring[x & 255] =
+// byte x of the row).
 template <bool WRITE>
-struct RleRow {
-  int prev[4], run[4], lit[4], lst[4];
-  long long pos[4], lim[4];
-  const uint8_t* row;   // the row's first pixel (literal bytes are re-read from here)
-  unsigned order;
+struct RleChan {
+  int prev, run, lit, lst;
+  long long pos, lim;
+  uint8_t* ring;
   uint8_t* out;
 
-  __device__ __forceinline__ void put(int s, unsigned v) {
-    if (WRITE && pos[s] < lim[s]) out[pos[s]] = (uint8_t)v;
-    ++pos[s];
+  __device__ __forceinline__ void put(unsigned v) {
+    if (WRITE && pos < lim) out[pos] = (uint8_t)v;
+    ++pos;
   }
-  __device__ __forceinline__ void literal(int s, int start, int k) {
-    if (!WRITE) { pos[s] += 1 + k; return; }
-    put(s, (unsigned)(k - 1));
-    const int b = (order >> (8 * s)) & 3;
-    for (int j = 0; j < k; ++j) put(s, row[(long long)(start + j) * 4 + b]);
+  __device__ __forceinline__ void literal(int start, int k) {
+    if (!WRITE) { pos += 1 + k; return; }
+    put((unsigned)(k - 1));
+    for (int j = 0; j < k; ++j) put(ring[(start + j) & (kRleRing - 1)]);
   }
-  // Closes the run of run[s] bytes equal to prev[s] that ends before x = end.
-  __device__ __forceinline__ void close(int s, int end) {
-    const int L = run[s];
+  // Closes the run of `run` bytes equal to prev that ends before x = end.
+  __device__ __forceinline__ void close(int end) {
+    const int L = run;
     if (L >= 3) {
-      if (lit[s] > 0) literal(s, lst[s], lit[s]);
-      lit[s] = 0;
-      lst[s] = end;
-      if (!WRITE) { pos[s] += 2 * ((L + 127) >> 7); return; }
+      // the pending literal segment went out when the run reached three bytes
+      lst = end;
+      if (!WRITE) { pos += 2 * ((L + 127) >> 7); return; }
       for (int rem = L; rem > 0; rem -= 128) {
         const int k = min(rem, 128);
-        put(s, k >= 2 ? (unsigned)(1 - k) & 0xFFu : 0u);
-        put(s, (unsigned)prev[s]);
+        put(k >= 2 ? (unsigned)(1 - k) & 0xFFu : 0u);
+        put((unsigned)prev);
       }
     } else {
-      lit[s] += L;
-      if (lit[s] >= 128) {
-        literal(s, lst[s], 128);
-        lst[s] += 128;
-        lit[s] -= 128;
+      lit += L;
+      if (lit >= 128) {
+        literal(lst, 128);
+        lst += 128;
+        lit -= 128;
       }
     }
   }
-  __device__ __forceinline__ void push(int s, int v, int x) {
-    if (v == prev[s]) { ++run[s]; return; }
-    close(s, x);
-    prev[s] = v;
-    run[s] = 1;
+  __device__ __forceinline__ void push(int v, int x) {
+    if (v == prev) {
+      if (++run == 3 && lit > 0) {   // this run will be replicate packets: the literals before it go now
+        literal(lst, lit);
+        lit = 0;
+      }
+      return;
+    }
+    close(x);
+    prev = v;
+    run = 1;
   }
-  __device__ __forceinline__ void finish(int s, int w) {
-    close(s, w);
-    if (lit[s] > 0) literal(s, lst[s], lit[s]);
+  __device__ __forceinline__ void finish(int w) {
+    close(w);
+    if (lit > 0) literal(lst, lit);
   }
 };
 
 template <bool WRITE>
-__global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
-  __shared__ uint32_t stage[kRleWarps][32 * kRlePitch];
-  const int lane = threadIdx.x & 31;
-  uint32_t* sm = stage[threadIdx.x >> 5];
-  const long long nwarps = (long long)gridDim.x * kRleWarps;
-  for (long long g = (long long)blockIdx.x * kRleWarps + (threadIdx.x >> 5); g < a.G; g += nwarps) {
-    int lo = 0, hi = a.N;   // largest i with group_base[i] <= g
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (a.group_base[mid] <= g) lo = mid; else hi = mid;
+__global__ void __launch_bounds__(kRleThreads) psd_rle_kernel(RleArgs a) {
+  __shared__ uint32_t stage[kRleRows * kRlePitch];
+  __shared__ __align__(16) uint8_t ring[WRITE ? kRleThreads * kRleRingPitch : 16];
+  __shared__ unsigned short s_planned[kRleRows * 4];
+  __shared__ int s_tot[4];
+  __shared__ int s_any;
+  __shared__ int s_layer;
+  const int t = threadIdx.x;
+  const int row = t >> 2, slot = t & 3;          // the four threads of a row are adjacent lanes
+  const int byte = (a.order >> (8 * slot)) & 3;   // which RGBA byte this thread's channel slot takes
+  for (long long g = blockIdx.x; g < a.G; g += gridDim.x) {
+    __syncthreads();   // the previous group is done with the shared buffers
+    if (t == 0) {
+      int lo = 0, hi = a.N;   // largest i with group_base[i] <= g
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (a.group_base[mid] <= g) lo = mid; else hi = mid;
+      }
+      s_layer = lo;
+      s_any = 0;
     }
-    const int i = lo;
+    if (t < 4) s_tot[t] = 0;
+    __syncthreads();
+    const int i = s_layer;
     const int w = a.sizes[2 * i], h = a.sizes[2 * i + 1];
     const long long off = a.layer_off[i];
     const bool ok = w >= 1 && w <= a.width_limit && h >= 1 && off >= 0 && (off & 3) == 0;
-    const long long y0 = (g - a.group_base[i]) * 32;
-    const int y = (int)y0 + lane;
-    const bool active = ok && y0 + lane < h;
+    const long long y0 = (g - a.group_base[i]) * kRleRows;
+    const long long y = y0 + row;
+    const bool active = ok && y < h;
     const uint8_t* base = a.layers + (ok ? off : 0);
 
-    RleRow<WRITE> e;
-    e.order = a.order;
+    RleChan<WRITE> e;
+    e.prev = -1; e.run = 0; e.lit = 0; e.lst = 0;
+    e.pos = 0; e.lim = 0;
+    e.ring = ring + (WRITE ? t * kRleRingPitch : 0);
     e.out = a.out;
-    e.row = base + (active ? (long long)y * w * 4 : 0);
-    unsigned short planned[4] = {0, 0, 0, 0};
-    bool skip = !ok;
+    bool skip = !ok;   // CTA-uniform: depends on the layer only
     if (WRITE) {
-      if (ok && active) {
-        const ushort4 rb = reinterpret_cast<const ushort4*>(a.row_bytes)[g * 32 + lane];
-        planned[0] = rb.x; planned[1] = rb.y; planned[2] = rb.z; planned[3] = rb.w;
-      }
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        int pre = planned[s];   // exclusive prefix over the group's rows
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, pre, d);
-          if (lane >= d) pre += t;
-        }
-        pre -= planned[s];
-        const long long co = ok ? a.chan_off[4 * i + s] : -1;
-        const long long gd = ok ? a.group_dst[4 * g + s] : -1;
-        if (co < 0 || gd < 0) {
-          e.pos[s] = 0; e.lim[s] = 0;   // every store of this slot is dropped
-        } else {
-          e.pos[s] = gd + pre;
-          e.lim[s] = min(e.pos[s] + planned[s], a.out_bytes);
-          if (active) {   // row byte count, big-endian, in the block's table; block header on row 0
-            const long long t = co + 2 + 2ll * y;
-            if (t + 1 < a.out_bytes) { a.out[t] = (uint8_t)(planned[s] >> 8); a.out[t + 1] = (uint8_t)planned[s]; }
-            if (y == 0 && co + 1 < a.out_bytes) { a.out[co] = 0; a.out[co + 1] = 1; }
-          }
+      const unsigned short planned = (ok && active) ? a.row_bytes[(g * kRleRows + row) * 4 + slot] : 0;
+      s_planned[row * 4 + slot] = planned;
+      __syncthreads();
+      long long pre = 0;   // exclusive prefix over the group's rows of this channel slot
+      for (int r = 0; r < row; ++r) pre += s_planned[r * 4 + slot];
+      const long long co = ok ? a.chan_off[4 * i + slot] : -1;
+      const long long gd = ok ? a.group_dst[4 * g + slot] : -1;
+      if (co >= 0 && gd >= 0) {
+        e.pos = gd + pre;
+        e.lim = min(e.pos + planned, a.out_bytes);
+        if (active) {   // row byte count, big-endian, in the block's table; block header on row 0
+          const long long tb = co + 2 + 2ll * y;
+          if (tb + 1 < a.out_bytes) { a.out[tb] = (uint8_t)(planned >> 8); a.out[tb + 1] = (uint8_t)planned; }
+          if (y == 0 && co + 1 < a.out_bytes) { a.out[co] = 0; a.out[co + 1] = 1; }
         }
       }
       skip = skip || (a.chan_off[4 * i] < 0 && a.chan_off[4 * i + 1] < 0 && a.chan_off[4 * i + 2] < 0 &&
                       a.chan_off[4 * i + 3] < 0);
-    } else {
-#pragma unroll
-      for (int s = 0; s < 4; ++s) { e.pos[s] = 0; e.lim[s] = 0; }
     }
-#pragma unroll
-    for (int s = 0; s < 4; ++s) { e.prev[s] = -1; e.run[s] = 0; e.lit[s] = 0; e.lst[s] = 0; }
 
-    uint32_t any_alpha = 0;
-    unsigned long long last = 1ull << 32;   // the previous pixel; no pixel equals the initial value
-    if (!skip) {   // warp-uniform: skip depends on the layer only
+    unsigned any_alpha = 0;
+    if (!skip) {
       for (int x0 = 0; x0 < w; x0 += 32) {
-        __syncwarp();
-#pragma unroll 4
-        for (int r = 0; r < 32; ++r) {
+        __syncthreads();
+        for (int k = t; k < kRleRows * 32; k += kRleThreads) {   // consecutive threads, consecutive pixels
+          const int r = k >> 5, c = k & 31;
           uint32_t v = 0;
-          if (y0 + r < h && x0 + lane < w)
-            v = *reinterpret_cast<const uint32_t*>(base + ((y0 + r) * (long long)w + x0 + lane) * 4);
-          sm[r * kRlePitch + lane] = v;
+          if (y0 + r < h && x0 + c < w)
+            v = *reinterpret_cast<const uint32_t*>(base + ((y0 + r) * (long long)w + x0 + c) * 4);
+          stage[r * kRlePitch + c] = v;
         }
-        __syncwarp();
+        __syncthreads();
         if (active) {
           const int n = min(32, w - x0);
+          const uint32_t* src = stage + row * kRlePitch;
           for (int x = 0; x < n; ++x) {
-            const uint32_t p = sm[lane * kRlePitch + x];
-            // Count pass only: when all four bytes repeat, every run grows.  The
-            // write pass measured slower with this shortcut (24.7 -> 28.3 ms at
-            // 2048x2048, N=20000 on a B200) and the count pass faster (12.5 ->
-            // 8.2 ms); both give the same bytes.
-            if (!WRITE && (unsigned long long)p == last) {
-#pragma unroll
-              for (int s = 0; s < 4; ++s) ++e.run[s];
-              continue;
-            }
-            if (!WRITE) last = p;
-            any_alpha |= p & 0xFF000000u;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) e.push(s, (p >> (8 * ((a.order >> (8 * s)) & 3))) & 0xFF, x0 + x);
+            const uint32_t p = src[x];
+            const int v = (p >> (8 * byte)) & 0xFF;
+            any_alpha |= p >> 24;
+            if (WRITE) e.ring[(x0 + x) & (kRleRing - 1)] = (uint8_t)v;
+            e.push(v, x0 + x);
           }
         }
       }
-      if (active) {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) e.finish(s, w);
-      }
+      if (active) e.finish(w);
     }
     if (!WRITE) {
-      int c[4];
-#pragma unroll
-      for (int s = 0; s < 4; ++s) c[s] = active && !skip ? (int)e.pos[s] : 0;
-      reinterpret_cast<ushort4*>(a.row_bytes)[g * 32 + lane] =
-          make_ushort4((unsigned short)c[0], (unsigned short)c[1], (unsigned short)c[2], (unsigned short)c[3]);
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) c[s] += __shfl_xor_sync(0xffffffffu, c[s], d);
+      const int c = active && !skip ? (int)e.pos : 0;
+      a.row_bytes[(g * kRleRows + row) * 4 + slot] = (unsigned short)c;
+      atomicAdd(&s_tot[slot], c);
+      if (any_alpha != 0) s_any = 1;
+      __syncthreads();
+      if (t == 0) {
+        reinterpret_cast<int4*>(a.group_tot)[g] = make_int4(s_tot[0], s_tot[1], s_tot[2], s_tot[3]);
+        if (s_any && a.alpha_any) a.alpha_any[i] = 1;
       }
-      if (lane == 0) reinterpret_cast<int4*>(a.group_tot)[g] = make_int4(c[0], c[1], c[2], c[3]);
-      if (__any_sync(0xffffffffu, any_alpha != 0) && lane == 0 && a.alpha_any) a.alpha_any[i] = 1;
     }
   }
 }
@@ -469,8 +466,8 @@ static int rle_resident_ctas(bool write) {
   if (r == 0) {
     int per_sm = 0, sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (write) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<true>, kRleWarps * 32, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<false>, kRleWarps * 32, 0);
+    if (write) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<true>, kRleThreads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psd_rle_kernel<false>, kRleThreads, 0);
     r = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 148);
   }
   return r;
@@ -483,13 +480,11 @@ int launch_psd_rle(bool write, const uint8_t* layers, const int* sizes, const lo
   if (G == 0 || N == 0) return DBMP_OK;
   const RleArgs a{layers, sizes, layer_off, group_base, G, N, order, width_limit, row_bytes, group_tot,
                   alpha_any, chan_off, group_dst, out, out_bytes};
-  // Persistent grid: as many CTAs as are resident at once (the device's SMs x
-  // the kernel's occupancy), so the grid-stride loop balances the row groups.
+  // persistent grid: as many CTAs as are resident at once, striding over the row groups
   const int resident = rle_resident_ctas(write);
-  long long ctas = (G + kRleWarps - 1) / kRleWarps;
-  if (ctas > resident) ctas = resident;
-  if (write) psd_rle_kernel<true><<<(int)ctas, kRleWarps * 32, 0, st>>>(a);
-  else psd_rle_kernel<false><<<(int)ctas, kRleWarps * 32, 0, st>>>(a);
+  const long long ctas = G < resident ? G : resident;
+  if (write) psd_rle_kernel<true><<<(int)ctas, kRleThreads, 0, st>>>(a);
+  else psd_rle_kernel<false><<<(int)ctas, kRleThreads, 0, st>>>(a);
   DBMP_CHECK_LAUNCH("psd_rle_kernel");
   return DBMP_OK;
 }
