@@ -408,8 +408,9 @@ def run_serving(n_jobs, seed, torch, subsample=5, load=0.8):
     res = srv.run(reqs, realtime=True)
     lat = serving.summarize(res)
     sub = reqs[::subsample]
-    seq_plain, t_plain = serving.run_sequential(sub, t_atlas, kind="f32", fused=False, graphs=True)
-    seq_fused, t_fused = serving.run_sequential(sub, t_atlas, kind=HEADLINE_KIND, fused=True, graphs=True)
+    seq_plain, t_plain, _ = serving.run_sequential(sub, t_atlas, kind="f32", fused=False, graphs=True)
+    seq_fused, t_fused, dev_fused = serving.run_sequential(sub, t_atlas, kind=HEADLINE_KIND, fused=True, graphs=True)
+    device_rate = len(sub) / dev_fused          # the fused jobs' iterations alone
     plain_rate, fused_rate = len(sub) / t_plain, len(sub) / t_fused
     served = {r.job_id: r.loss for r in res}
     d_fused = max(abs(served[q.job_id] - f.loss) / max(abs(f.loss), 1e-30) for q, f in zip(sub, seq_fused))
@@ -420,6 +421,9 @@ def run_serving(n_jobs, seed, torch, subsample=5, load=0.8):
             "mean_final_l2": lat["mean_loss"], "replayed_steps": cap["replayed"] + lat["replayed"],
             "sequential_plain_fp32_graphed_jobs_per_s": plain_rate,
             "sequential_fused_f16_graphed_jobs_per_s": fused_rate,
+            "fused_f16_iterations_only_jobs_per_s": device_rate,
+            "fused_f16_iterations_only_note": "the same jobs' 100 iterations each, one job at a time, device time "
+                                              "(CUDA events) without set-up or host waits",
             "baseline_sample": f"every {subsample}th job of the stream ({len(sub)} jobs), one at a time",
             "capacity_vs_sequential_plain_fp32": cap["jobs_per_s"] / plain_rate,
             "capacity_vs_sequential_fused_f16": cap["jobs_per_s"] / fused_rate,
@@ -778,16 +782,23 @@ def main():
         torch.cuda.empty_cache()          # the serving loop's cached blocks belong to its streams
         line["psd"] = run_psd(torch, peaks)
     if rank == 0 and world == 1 and not args.fast:
-        ref = CpuReference(spec)
-        rows = ref.rows_for_budget(15.0)          # about 15 s of CPU work
-        t_cpu = ref.sample(rows)
         # the same leg renders the precision band with the FP64 oracle, the
         # checker of the storage kinds' images rendered above
         line["precision"] = precision_vs_oracle(spec, band, renders)
-        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "iters/s", "cores": os.cpu_count(),
-                                "kind": "port",
-                                "sample": f"oracle fwd+bwd (reference algorithm, FP64, no termination) on {rows} of "
-                                          f"{spec.H} pixel rows, extrapolated to the canvas"}
+        ref = TorchReference(spec)
+        k = ref.tiles_for_budget(15.0)           # about 15 s of CPU work
+        t_cpu = ref.sample(k)
+        port = CpuReference(spec)
+        rows = port.rows_for_budget(4.0)
+        t_port = port.sample(rows)
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "iters/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"fwd+bwd of the reference's PyTorch per-tile renderer (restated, pinned "
+                                          f"to its outputs) on {k} of {ref.T} tiles, evenly spaced, extrapolated "
+                                          f"to the canvas by tile count",
+                                "fp64_port": {"value": 1.0 / t_port, "unit": "iters/s",
+                                              "sample": f"FP64 restatement of the reference kernels' algorithm "
+                                                        f"(no termination), fwd+bwd on {rows} of {spec.H} pixel "
+                                                        f"rows, extrapolated"}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

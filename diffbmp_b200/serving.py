@@ -274,10 +274,12 @@ def run_sequential(requests: List[JobRequest], atlas_templates, kind="f32", fuse
     """One job at a time, to completion: the baselines of the serving target.
     Each job is set up as the server sets one up (lists sized from
     list_capacity_bound, the iteration captured in a CUDA graph when
-    `graphs`), then runs its iterations and reads its result."""
+    `graphs`), then runs its iterations and reads its result.  Returns
+    (results, wall seconds, device seconds of the iterations alone)."""
     atlas = Atlas(atlas_templates, kind)
     cfg = FitConfig(lr=lr, fused=fused)
     out = []
+    device_s = 0.0
     t0 = time.perf_counter()
     for req in requests:
         s = req.spec
@@ -285,8 +287,12 @@ def run_sequential(requests: List[JobRequest], atlas_templates, kind="f32", fuse
                         s.background, cfg, list_capacity=list_capacity_bound(s, cfg.tile_size))
         if graphs:
             f.capture()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         for _ in range(req.iterations):
             f.step()
+        e1.record()
         rep = f.sync()
+        device_s += e0.elapsed_time(e1) / 1e3
         out.append(JobResult(req.job_id, 0.0, 0.0, time.perf_counter() - t0, f.loss(), rep))
-    return out, time.perf_counter() - t0
+    return out, time.perf_counter() - t0, device_s
