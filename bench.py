@@ -679,9 +679,10 @@ def main():
     losses = []
 
     def e2e_step(i):
-        # one step in flight: step i is enqueued (inputs H2D, iteration, loss
-        # D2H), then the host waits for step i - 1 and reads its loss
-        dev_params.copy_(host, non_blocking=True)
+        # one step in flight: step i is enqueued (inputs H2D through the
+        # double-buffered upload, iteration, loss D2H), then the host waits for
+        # step i - 1 and reads its loss
+        e2e_job.upload_params(host)
         e2e_job.step()
         loss_host[i % 2:i % 2 + 1].copy_(e2e_job.loss_dev, non_blocking=True)
         done[i % 2].record()
@@ -762,8 +763,9 @@ def main():
                      "hbm_peak_gbs_measured": peaks.get("hbm_gbs")},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 8,
-                "what": "public API: params H2D from pinned host, ImageFitter.step(), loss D2H read by the host "
-                        "every step, one step in flight"},
+                "what": "public API: every step's parameters H2D from pinned host (ImageFitter.upload_params: copy "
+                        "stream, two staging buffers), ImageFitter.step(), loss D2H read by the host every step, "
+                        "one step in flight"},
         "gpu_launches": 6 * args.steps,
         "gpu_launches_note": "ours per step: prepare, counts, bin_rows, fused, adam, step_increment "
                              "(+ one memset and the two kernels of one CUB exclusive scan over the tile counts)",

@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
   float x = 0.f, y = 0.f, r = 0.f, theta = 0.f, cos_t = 0.f, sin_t = 0.f, vs = 0.f, cr = 0.f, cg = 0.f, cb = 0.f;
   int t_idx = 0, bx_n = 1;
   long long off = 0, first = 0;    // the layer's byte offset and first block
+  int bx = 0, by = 0;              // the current block's first pixel within the crop
   for (long long b = b0; b < b1; ++b) {
     bool changed = false;
     if (lane == 0 && (n < 0 || b >= next)) {
@@ -225,10 +226,15 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
       off = __shfl_sync(0xffffffffu, off, 0);
       first = __shfl_sync(0xffffffffu, first, 0);
       bx_n = __shfl_sync(0xffffffffu, bx_n, 0);
+      const int k = (int)(b - first);   // block within the crop (a crop has < 2^31 blocks)
+      bx = (k % bx_n) * kPsdBlock;
+      by = (k / bx_n) * kPsdBlock;
+    } else {                            // the next block of the same crop, row-major
+      bx += kPsdBlock;
+      if (bx >= bb.z - bb.x) { bx = 0; by += kPsdBlock; }
     }
-    const int k = (int)(b - first);   // block within the crop (a crop has < 2^31 blocks)
     const int bw = bb.z - bb.x, bh = bb.w - bb.y;
-    const int lpx = (k % bx_n) * kPsdBlock + lx, lpy = (k / bx_n) * kPsdBlock + ly;
+    const int lpx = bx + lx, lpy = by + ly;
     if (lpx >= bw || lpy >= bh) continue;
     const int px = bb.x + lpx, py = bb.y + lpy;
     const float tv = psd_template_value(tmpl, t_idx, a.P, a.Ht, a.Wt, px, py, x, y, r, cos_t, sin_t);

@@ -338,6 +338,36 @@ class ImageFitter:
              _ptr(self.radii), _ptr(self.rotations), _ptr(self.opacities), _ptr(self.colors), _ptr(self.adam_m),
              _ptr(self.adam_v), _ptr(self.step_count), skip, st)
 
+    def upload_params(self, host_params: torch.Tensor):
+        """Sets the parameters from a pinned host tensor laid out as
+        params_flat ((N*8,) f32: centres, radii, rotations, opacity and colour
+        logits), without stalling the device: the host-to-device copy runs on
+        a copy stream into one of two staging buffers, so it overlaps the work
+        already queued, and the current stream only waits for it and copies
+        device to device before the next step reads the parameters."""
+        if host_params.numel() != self.params_flat.numel():
+            raise ValueError(f"{host_params.numel()} values for {self.params_flat.numel()} parameters")
+        if not hasattr(self, "_staging"):
+            self._copy_stream = torch.cuda.Stream(self.device)
+            self._staging = [torch.empty_like(self.params_flat) for _ in range(2)]
+            self._staged = [torch.cuda.Event(), torch.cuda.Event()]
+            self._consumed = [None, None]
+            self._slot = 0
+        k = self._slot
+        self._slot ^= 1
+        cs = self._copy_stream
+        if self._consumed[k] is not None:          # the device copy that last read this buffer is done
+            cs.wait_event(self._consumed[k])
+        with torch.cuda.stream(cs):
+            self._staging[k].copy_(host_params.view(-1), non_blocking=True)
+        self._staged[k].record(cs)
+        cur = torch.cuda.current_stream(self.device)
+        cur.wait_event(self._staged[k])
+        self.params_flat.copy_(self._staging[k], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        self._consumed[k] = ev
+
     def step(self):
         """Enqueues one fit iteration (no host synchronisation)."""
         if self.graph is not None:

@@ -200,3 +200,22 @@ def test_loop_decay_blur_prune_step_by_step():
             torch.testing.assert_close(job.params()[key], ref[key].detach(), rtol=2e-5, atol=2e-5,
                                        msg=lambda m, key=key: f"iteration {k}, {key}: {m}")
     assert replaced > 0 and int(job.prune_state[3].item()) == replaced
+
+
+def test_upload_params_double_buffered(spec):
+    """ImageFitter.upload_params (copy stream, two staging buffers) gives
+    each step the parameters uploaded for it, like a plain copy before the step."""
+    a, b = make(spec), make(spec)
+    rng = np.random.default_rng(8)
+    base = a.params_flat.cpu()
+    hosts = [(base + torch.from_numpy(rng.normal(0, 0.5, base.shape).astype(np.float32))).pin_memory()
+             for _ in range(3)]
+    a.capture()
+    for h in hosts:
+        a.upload_params(h)
+        a.step()
+        b.params_flat.copy_(h.cuda())
+        b.step()
+    a.sync(); b.sync()
+    assert torch.equal(a.params_flat, b.params_flat)
+    assert abs(a.loss() - b.loss()) <= 1e-12 * max(1.0, abs(b.loss()))
