@@ -323,14 +323,19 @@ __global__ void __launch_bounds__(1024) counts_kernel(Geom g, BinGrid bg, int* _
   if (slice == 0 && threadIdx.x == 0) counts[(long long)g.T * bg.slices] = 0;
 }
 
-__global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid bg, const int4* __restrict__ rects,
-                                                               const long long* __restrict__ offs, long long cap,
-                                                               int* __restrict__ indices,
-                                                               int* __restrict__ tile_offsets,
-                                                               int* __restrict__ total_out,
-                                                               int* __restrict__ overflow_out) {
-  __shared__ int s_id[kBinThreads], s_x0[kBinThreads], s_x1[kBinThreads];
-  __shared__ int s_wcnt[kBinGroup];
+__global__ void __launch_bounds__(kBinThreads, 4) bin_rows_kernel(Geom g, BinGrid bg,
+                                                                  const int4* __restrict__ rects,
+                                                                  const long long* __restrict__ offs, long long cap,
+                                                                  int* __restrict__ indices,
+                                                                  int* __restrict__ tile_offsets,
+                                                                  int* __restrict__ total_out,
+                                                                  int* __restrict__ overflow_out) {
+  // Two compaction buffers: chunk c is compacted into buffer c & 1 while the
+  // warps may still read chunk c - 1 from the other one, so one barrier per
+  // chunk orders everything (see the loop).
+  __shared__ int s_id[2][kBinThreads];
+  __shared__ int2 s_xr[2][kBinThreads];   // the rectangle's tile columns x0, x1
+  __shared__ int s_wcnt[2][kBinGroup];
   const int slice = blockIdx.x % bg.slices;
   const int rg = blockIdx.x / bg.slices;
   const int ty = rg / bg.groups;
@@ -350,7 +355,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid b
       if (total_out) *total_out = (int)min(L, (long long)INT_MAX);
       if (overflow_out) *overflow_out = (L > cap) ? 1 : 0;
     }
-    if (L > cap) return;
+    if (L > cap) return;   // uniform over the CTA
     if (first) tile_offsets[g.T] = (int)L;
     if (has_tile) {
       cur = offs[slot];
@@ -358,39 +363,56 @@ __global__ void __launch_bounds__(kBinThreads) bin_rows_kernel(Geom g, BinGrid b
     }
   }
   const int lo = slice * bg.span, hi = min(g.N, lo + bg.span);
-  int4 rc = make_int4(1, 0, 1, 0);
-  if (lo + (int)threadIdx.x < hi) rc = rects[lo + threadIdx.x];
-  for (int base = lo; base < hi; base += kBinThreads) {
-    const int n = base + threadIdx.x;
-    // prefetch the next chunk's rectangle while this one is processed
-    int4 rn = make_int4(1, 0, 1, 0);
-    if (n + kBinThreads < hi) rn = rects[n + kBinThreads];
-    const bool f = n < hi && rc.x <= rc.y && rc.z <= ty && ty <= rc.w && rc.x <= gx1 && rc.y >= gx0;
-    const unsigned b = __ballot_sync(0xffffffffu, f);
-    if (lane == 0) s_wcnt[warp] = __popc(b);
-    __syncthreads();
-    int wbase = 0, total = 0;
+  const int4 none = make_int4(1, 0, 1, 0);
+  // a rectangle survives the CTA's test when it covers row ty and overlaps the tile group
+  auto covers = [&](const int4& rc) { return rc.x <= rc.y && rc.z <= ty && ty <= rc.w && rc.x <= gx1 && rc.y >= gx0; };
+  // chunk lo: test, count; the rectangles of the next chunk are loaded one chunk ahead
+  int n = lo + (int)threadIdx.x;
+  int4 rc = n < hi ? rects[n] : none;
+  int4 rn = n + kBinThreads < hi ? rects[n + kBinThreads] : none;
+  bool f = n < hi && covers(rc);
+  unsigned b = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) s_wcnt[0][warp] = __popc(b);
+  __syncthreads();
+  int buf = 0;
+  for (int base = lo; base < hi; base += kBinThreads, buf ^= 1) {
+    // (1) compact chunk base into buffer buf (its counts were published before
+    // the last barrier): lane w < kBinGroup scans the counts of warps 0..w
+    int inc = lane < kBinGroup ? s_wcnt[buf][lane] : 0;
 #pragma unroll
-    for (int w = 0; w < kBinGroup; ++w) {
-      const int c = s_wcnt[w];
-      wbase += (w < warp) ? c : 0;
-      total += c;
+    for (int o = 1; o < kBinGroup; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
     }
+    const int total = __shfl_sync(0xffffffffu, inc, kBinGroup - 1);
+    const int wbase = warp == 0 ? 0 : __shfl_sync(0xffffffffu, inc, warp - 1);
     if (f) {
       const int p = wbase + __popc(b & lt);
-      s_id[p] = n; s_x0[p] = rc.x; s_x1[p] = rc.y;
+      s_id[buf][p] = n;
+      s_xr[buf][p] = make_int2(rc.x, rc.y);
     }
+    // (2) test and count the next chunk, and load the one after it
+    n += kBinThreads;
+    rc = rn;
+    rn = n + kBinThreads < hi ? rects[n + kBinThreads] : none;
+    f = n < hi && covers(rc);
+    b = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) s_wcnt[buf ^ 1][warp] = __popc(b);
+    // One barrier per chunk.  After it, buffer buf holds chunk base and
+    // s_wcnt[buf ^ 1] the next chunk's counts.  The next iteration writes
+    // buffer buf ^ 1, last read by this iteration's predecessor (before this
+    // barrier), and s_wcnt[buf], last read in (1) above (before this barrier).
     __syncthreads();
+    // (3) each warp writes the compacted rectangles that contain its tile
     if (has_tile) {
       for (int j = lane; j < ((total + 31) & ~31); j += 32) {
-        const bool in = j < total && s_x0[j] <= tx && tx <= s_x1[j];
+        const int2 xr = j < total ? s_xr[buf][j] : make_int2(1, 0);
+        const bool in = xr.x <= tx && tx <= xr.y;
         const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) indices[cur + __popc(m & lt)] = s_id[j];
+        if (in) indices[cur + __popc(m & lt)] = s_id[buf][j];
         cur += __popc(m);
       }
     }
-    __syncthreads();   // the compacted chunk is reused by the next iteration
-    rc = rn;
   }
 }
 
