@@ -244,15 +244,20 @@ __global__ void prepare_kernel(Geom g, const float* __restrict__ means2D, const 
 // it into counts[t * S + slice], the number of the slice's rectangles covering
 // tile t.  The exclusive scan of the counts is tile-major and slice-minor.
 // Write: one CTA per (tile row, group of kBinGroup tiles, primitive slice),
-// one warp per tile; the CTA walks the primitives of its slice in index order
-// in chunks of kBinThreads, compacts those whose rectangle covers its row and
-// overlaps its tile group, and each warp writes the ids of the compacted
-// rectangles containing its tile from offs[t * S + slice] on, so a tile's
-// entries come out in ascending primitive order.  The write pass also
+// kBinTPW tiles per warp (warp w: tiles w + k kBinWarps of the group); the
+// CTA walks the primitives of its slice in index order in chunks of
+// kBinThreads, compacts those whose rectangle covers its row and overlaps its
+// tile group, and each warp writes the ids of the compacted rectangles
+// containing each of its tiles from offs[t * S + slice] on, so a tile's
+// entries come out in ascending primitive order.  Two tiles per warp halve
+// the per-tile share of the row filter, compaction and count scan (write
+// pass 39.8 -> 29.4 us at 2048x2048, N=20000 on a B200).  The write pass also
 // publishes tile_offsets, L and the overflow flag, and leaves the outputs
 // untouched when L exceeds the capacity.
 constexpr int kBinThreads = 512;
-constexpr int kBinGroup = kBinThreads / 32;
+constexpr int kBinWarps = kBinThreads / 32;
+constexpr int kBinTPW = 2;                       // tiles per warp
+constexpr int kBinGroup = kBinTPW * kBinWarps;   // tiles per CTA
 
 struct BinGrid {
   int groups;   // tile groups per row
@@ -323,7 +328,7 @@ __global__ void __launch_bounds__(1024) counts_kernel(Geom g, BinGrid bg, int* _
   if (slice == 0 && threadIdx.x == 0) counts[(long long)g.T * bg.slices] = 0;
 }
 
-__global__ void __launch_bounds__(kBinThreads, 4) bin_rows_kernel(Geom g, BinGrid bg,
+__global__ void __launch_bounds__(kBinThreads, 3) bin_rows_kernel(Geom g, BinGrid bg,
                                                                   const int4* __restrict__ rects,
                                                                   const long long* __restrict__ offs, long long cap,
                                                                   int* __restrict__ indices,
@@ -335,19 +340,19 @@ __global__ void __launch_bounds__(kBinThreads, 4) bin_rows_kernel(Geom g, BinGri
   // chunk orders everything (see the loop).
   __shared__ int s_id[2][kBinThreads];
   __shared__ int2 s_xr[2][kBinThreads];   // the rectangle's tile columns x0, x1
-  __shared__ int s_wcnt[2][kBinGroup];
+  __shared__ int s_wcnt[2][kBinWarps];
   const int slice = blockIdx.x % bg.slices;
   const int rg = blockIdx.x / bg.slices;
   const int ty = rg / bg.groups;
   const int gx0 = (rg - ty * bg.groups) * kBinGroup, gx1 = min(gx0 + kBinGroup - 1, g.tilesX - 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tx = gx0 + warp;
-  const bool has_tile = tx <= gx1;
-  const int t = ty * g.tilesX + tx;
-  const long long slot = (long long)t * bg.slices + slice;
   const long long nslots = (long long)g.T * bg.slices;
   const unsigned lt = (1u << lane) - 1u;
-  long long cur = 0;
+  // this warp's tiles gx0 + warp + k kBinWarps: the column a rectangle must
+  // reach (INT_MAX for a tile past the canvas, which no rectangle contains)
+  // and the next write position of each
+  int col[kBinTPW];
+  long long cur[kBinTPW];
   {
     const long long L = offs[nslots];
     const bool first = blockIdx.x == 0 && threadIdx.x == 0;
@@ -357,9 +362,17 @@ __global__ void __launch_bounds__(kBinThreads, 4) bin_rows_kernel(Geom g, BinGri
     }
     if (L > cap) return;   // uniform over the CTA
     if (first) tile_offsets[g.T] = (int)L;
-    if (has_tile) {
-      cur = offs[slot];
-      if (lane == 0 && slice == 0) tile_offsets[t] = (int)cur;
+#pragma unroll
+    for (int k = 0; k < kBinTPW; ++k) {
+      const int tx = gx0 + warp + k * kBinWarps;
+      col[k] = INT_MAX;
+      cur[k] = 0;
+      if (tx <= gx1) {
+        const int t = ty * g.tilesX + tx;
+        col[k] = tx;
+        cur[k] = offs[(long long)t * bg.slices + slice];
+        if (lane == 0 && slice == 0) tile_offsets[t] = (int)cur[k];
+      }
     }
   }
   const int lo = slice * bg.span, hi = min(g.N, lo + bg.span);
@@ -377,14 +390,14 @@ __global__ void __launch_bounds__(kBinThreads, 4) bin_rows_kernel(Geom g, BinGri
   int buf = 0;
   for (int base = lo; base < hi; base += kBinThreads, buf ^= 1) {
     // (1) compact chunk base into buffer buf (its counts were published before
-    // the last barrier): lane w < kBinGroup scans the counts of warps 0..w
-    int inc = lane < kBinGroup ? s_wcnt[buf][lane] : 0;
+    // the last barrier): lane w < kBinWarps scans the counts of warps 0..w
+    int inc = lane < kBinWarps ? s_wcnt[buf][lane] : 0;
 #pragma unroll
-    for (int o = 1; o < kBinGroup; o <<= 1) {
+    for (int o = 1; o < kBinWarps; o <<= 1) {
       const int u = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += u;
     }
-    const int total = __shfl_sync(0xffffffffu, inc, kBinGroup - 1);
+    const int total = __shfl_sync(0xffffffffu, inc, kBinWarps - 1);
     const int wbase = warp == 0 ? 0 : __shfl_sync(0xffffffffu, inc, warp - 1);
     if (f) {
       const int p = wbase + __popc(b & lt);
@@ -403,14 +416,16 @@ __global__ void __launch_bounds__(kBinThreads, 4) bin_rows_kernel(Geom g, BinGri
     // buffer buf ^ 1, last read by this iteration's predecessor (before this
     // barrier), and s_wcnt[buf], last read in (1) above (before this barrier).
     __syncthreads();
-    // (3) each warp writes the compacted rectangles that contain its tile
-    if (has_tile) {
-      for (int j = lane; j < ((total + 31) & ~31); j += 32) {
-        const int2 xr = j < total ? s_xr[buf][j] : make_int2(1, 0);
-        const bool in = xr.x <= tx && tx <= xr.y;
+    // (3) each warp writes the compacted rectangles that contain its tiles
+    for (int j = lane; j < ((total + 31) & ~31); j += 32) {
+      const int2 xr = j < total ? s_xr[buf][j] : make_int2(1, 0);
+      const int id = j < total ? s_id[buf][j] : 0;
+#pragma unroll
+      for (int k = 0; k < kBinTPW; ++k) {
+        const bool in = xr.x <= col[k] && col[k] <= xr.y;
         const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) indices[cur + __popc(m & lt)] = s_id[buf][j];
-        cur += __popc(m);
+        if (in) indices[cur[k] + __popc(m & lt)] = id;
+        cur[k] += __popc(m);
       }
     }
   }

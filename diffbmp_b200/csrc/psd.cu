@@ -15,6 +15,7 @@
 #include <cstdint>
 
 #include <mutex>
+#include <type_traits>
 
 #include "dbmp_internal.cuh"
 
@@ -307,56 +308,93 @@ struct RleArgs {
   long long out_bytes;
 };
 
-// Four PackBits encoders of one row.  COUNT only adds sizes; WRITE stores.
-template <bool WRITE>
-struct RleRow {
-  int prev[4], run[4], lit[4], lst[4];
-  long long pos[4], lim[4];
-  const uint8_t* row;   // the row's first pixel (literal bytes are re-read from here)
-  unsigned order;
-  uint8_t* out;
+// Four PackBits encoders of one row, counting output bytes only (count pass).
+// A literal segment's headers are added when the segment closes, or when 128
+// bytes are in.
+struct RleCount {
+  int prev[4], run[4], lit[4];
+  long long pos[4];
 
-  __device__ __forceinline__ void put(int s, unsigned v) {
-    if (WRITE && pos[s] < lim[s]) out[pos[s]] = (uint8_t)v;
-    ++pos[s];
-  }
-  __device__ __forceinline__ void literal(int s, int start, int k) {
-    if (!WRITE) { pos[s] += 1 + k; return; }
-    put(s, (unsigned)(k - 1));
-    const int b = (order >> (8 * s)) & 3;
-    for (int j = 0; j < k; ++j) put(s, row[(long long)(start + j) * 4 + b]);
-  }
-  // Closes the run of run[s] bytes equal to prev[s] that ends before x = end.
-  __device__ __forceinline__ void close(int s, int end) {
+  __device__ __forceinline__ void close(int s) {
     const int L = run[s];
     if (L >= 3) {
-      if (lit[s] > 0) literal(s, lst[s], lit[s]);
+      if (lit[s] > 0) pos[s] += 1 + lit[s];
       lit[s] = 0;
-      lst[s] = end;
-      if (!WRITE) { pos[s] += 2 * ((L + 127) >> 7); return; }
+      pos[s] += 2 * ((L + 127) >> 7);
+    } else {
+      lit[s] += L;
+      if (lit[s] >= 128) {
+        pos[s] += 129;
+        lit[s] -= 128;
+      }
+    }
+  }
+  __device__ __forceinline__ void push(int s, int v) {
+    if (v == prev[s]) { ++run[s]; return; }
+    close(s);
+    prev[s] = v;
+    run[s] = 1;
+  }
+  __device__ __forceinline__ void finish(int s) {
+    close(s);
+    if (lit[s] > 0) pos[s] += 1 + lit[s];
+  }
+};
+
+// Four PackBits encoders of one row that store their bytes (write pass).
+// Positions are byte offsets within the row's output of each channel slot.
+// A literal byte is stored as soon as its run closes (a run of one or two
+// bytes), at its final place: a literal packet's header position is reserved
+// when the packet opens and written when it closes (127 when 128 bytes are
+// in, the count minus one at the end of the segment), so no byte of the crop
+// is read twice.  (An earlier form re-read literal bytes from the crop when
+// their segment closed: 23.3 against 14.9 ms at 2048x2048, N=20000.  The
+// count pass keeps its own encoder: sharing this one took it from 8.0 to
+// 14.1 ms.)
+struct RleWrite {
+  int prev[4], run[4], lit[4], pos[4], lim[4], hdr[4];
+  uint8_t* dst[4];   // the row's first output byte of each slot
+
+  __device__ __forceinline__ void store(int s, int p, unsigned v) {
+    if (p < lim[s]) dst[s][p] = (uint8_t)v;
+  }
+  __device__ __forceinline__ void put(int s, unsigned v) {
+    store(s, pos[s], v);
+    ++pos[s];
+  }
+  // Appends one byte to the open literal segment.
+  __device__ __forceinline__ void lit_byte(int s, unsigned v) {
+    if ((lit[s] & 127) == 0) hdr[s] = pos[s]++;
+    put(s, v);
+    if ((++lit[s] & 127) == 0) store(s, hdr[s], 127u);
+  }
+  __device__ __forceinline__ void end_literal(int s) {
+    if (lit[s] & 127) store(s, hdr[s], (unsigned)((lit[s] & 127) - 1));
+    lit[s] = 0;
+  }
+  // Closes the run of run[s] bytes equal to prev[s].
+  __device__ __forceinline__ void close(int s) {
+    const int L = run[s];
+    if (L >= 3) {
+      end_literal(s);
       for (int rem = L; rem > 0; rem -= 128) {
         const int k = min(rem, 128);
         put(s, k >= 2 ? (unsigned)(1 - k) & 0xFFu : 0u);
         put(s, (unsigned)prev[s]);
       }
     } else {
-      lit[s] += L;
-      if (lit[s] >= 128) {
-        literal(s, lst[s], 128);
-        lst[s] += 128;
-        lit[s] -= 128;
-      }
+      for (int j = 0; j < L; ++j) lit_byte(s, (unsigned)prev[s]);
     }
   }
-  __device__ __forceinline__ void push(int s, int v, int x) {
+  __device__ __forceinline__ void push(int s, int v) {
     if (v == prev[s]) { ++run[s]; return; }
-    close(s, x);
+    close(s);
     prev[s] = v;
     run[s] = 1;
   }
-  __device__ __forceinline__ void finish(int s, int w) {
-    close(s, w);
-    if (lit[s] > 0) literal(s, lst[s], lit[s]);
+  __device__ __forceinline__ void finish(int s) {
+    close(s);
+    end_literal(s);
   }
 };
 
@@ -381,13 +419,14 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
     const bool active = ok && y0 + lane < h;
     const uint8_t* base = a.layers + (ok ? off : 0);
 
-    RleRow<WRITE> e;
-    e.order = a.order;
-    e.out = a.out;
-    e.row = base + (active ? (long long)y * w * 4 : 0);
+    std::conditional_t<WRITE, RleWrite, RleCount> e;
     unsigned short planned[4] = {0, 0, 0, 0};
     bool skip = !ok;
-    if (WRITE) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) e.pos[s] = 0;
+    if constexpr (WRITE) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) { e.lim[s] = 0; e.hdr[s] = 0; e.dst[s] = a.out; }
       if (ok && active) {
         const ushort4 rb = reinterpret_cast<const ushort4*>(a.row_bytes)[g * 32 + lane];
         planned[0] = rb.x; planned[1] = rb.y; planned[2] = rb.z; planned[3] = rb.w;
@@ -403,11 +442,10 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
         pre -= planned[s];
         const long long co = ok ? a.chan_off[4 * i + s] : -1;
         const long long gd = ok ? a.group_dst[4 * g + s] : -1;
-        if (co < 0 || gd < 0) {
-          e.pos[s] = 0; e.lim[s] = 0;   // every store of this slot is dropped
-        } else {
-          e.pos[s] = gd + pre;
-          e.lim[s] = min(e.pos[s] + planned[s], a.out_bytes);
+        if (co >= 0 && gd >= 0) {   // otherwise every store of this slot is dropped
+          const long long start = gd + pre;
+          e.dst[s] = a.out + start;
+          e.lim[s] = (int)max(0ll, min((long long)planned[s], a.out_bytes - start));
           if (active) {   // row byte count, big-endian, in the block's table; block header on row 0
             const long long t = co + 2 + 2ll * y;
             if (t + 1 < a.out_bytes) { a.out[t] = (uint8_t)(planned[s] >> 8); a.out[t + 1] = (uint8_t)planned[s]; }
@@ -417,12 +455,9 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
       }
       skip = skip || (a.chan_off[4 * i] < 0 && a.chan_off[4 * i + 1] < 0 && a.chan_off[4 * i + 2] < 0 &&
                       a.chan_off[4 * i + 3] < 0);
-    } else {
-#pragma unroll
-      for (int s = 0; s < 4; ++s) { e.pos[s] = 0; e.lim[s] = 0; }
     }
 #pragma unroll
-    for (int s = 0; s < 4; ++s) { e.prev[s] = -1; e.run[s] = 0; e.lit[s] = 0; e.lst[s] = 0; }
+    for (int s = 0; s < 4; ++s) { e.prev[s] = -1; e.run[s] = 0; e.lit[s] = 0; }
 
     uint32_t any_alpha = 0;
     unsigned long long last = 1ull << 32;   // the previous pixel; no pixel equals the initial value
@@ -453,13 +488,13 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
             if (!WRITE) last = p;
             any_alpha |= p & 0xFF000000u;
 #pragma unroll
-            for (int s = 0; s < 4; ++s) e.push(s, (p >> (8 * ((a.order >> (8 * s)) & 3))) & 0xFF, x0 + x);
+            for (int s = 0; s < 4; ++s) e.push(s, (p >> (8 * ((a.order >> (8 * s)) & 3))) & 0xFF);
           }
         }
       }
       if (active) {
 #pragma unroll
-        for (int s = 0; s < 4; ++s) e.finish(s, w);
+        for (int s = 0; s < 4; ++s) e.finish(s);
       }
     }
     if (!WRITE) {
