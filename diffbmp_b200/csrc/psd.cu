@@ -152,14 +152,16 @@ struct PsdArgs {
 };
 
 // Stage 2 (psd_export_kernels.cu:61-198): the 16x16 blocks of all crops, block
-// b of layer n for blk[n] <= b < blk[n+1].  Each CTA takes a contiguous range
-// of blocks and each of its warps walks the range's blocks in order, 32
-// pixels (two block rows) of each; lane 0 of the warp follows the layer index
-// forward from block to block (a binary search only for the range's first
-// block) and loads the layer's box, centre, radius, rotation with its cosine
-// and sine, opacity and colour once per layer, broadcast to the lanes.  Each
-// thread then computes its pixel with the reference's per-pixel operations on
-// the same values, so the bytes are the ones a per-pixel evaluation gives.
+// b of layer n for blk[n] <= b < blk[n+1].  Each warp takes a contiguous range
+// of blocks and walks them in order, a whole block at a time: lane l owns
+// column l % 16 and rows l / 16, l / 16 + 2, ... of the block (eight pixels;
+// each half-warp stores 64 contiguous bytes of a row).  Lane 0 follows the
+// layer index forward from block to block (a binary search only for the
+// range's first block) and loads the layer's box, centre, radius, rotation
+// with its cosine and sine, opacity and colour once per layer, broadcast to
+// the lanes.  Each thread then computes its pixels with the reference's
+// per-pixel operations on the same values, so the bytes are the ones a
+// per-pixel evaluation gives.
 __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float* __restrict__ means2D,
                                                          const float* __restrict__ radii,
                                                          const float* __restrict__ rot,
@@ -172,10 +174,12 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
                                                          const float* __restrict__ colors_orig,
                                                          uint8_t* __restrict__ out) {
   const long long nblk = blk[a.N];
-  const long long per = (nblk + gridDim.x - 1) / gridDim.x;
-  const long long b0 = (long long)blockIdx.x * per, b1 = min(b0 + per, nblk);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lx = lane & (kPsdBlock - 1), ly = 2 * warp + (lane >> 4);   // this thread's pixel in a block
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long long per = (nblk + nwarps - 1) / nwarps;
+  const long long b0 = gw * per, b1 = min(b0 + per, nblk);
+  const int lx = lane & (kPsdBlock - 1), ly0 = lane >> 4;   // this thread's column and first row in a block
   int n = -1;                      // the current layer (lane 0's bookkeeping, broadcast below)
   long long next = 0;              // blk[n + 1]
   int4 bb = make_int4(0, 0, 0, 0);
@@ -235,28 +239,39 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
       if (bx >= bb.z - bb.x) { bx = 0; by += kPsdBlock; }
     }
     const int bw = bb.z - bb.x, bh = bb.w - bb.y;
-    const int lpx = bx + lx, lpy = by + ly;
-    if (lpx >= bw || lpy >= bh) continue;
-    const int px = bb.x + lpx, py = bb.y + lpy;
-    const float tv = psd_template_value(tmpl, t_idx, a.P, a.Ht, a.Wt, px, py, x, y, r, cos_t, sin_t);
-    const float alpha_val = tv * vs * a.alpha_max;
-    uchar4 px4 = make_uchar4(0, 0, 0, 0);
-    if (!(alpha_val < 0.001f)) {
-      float rgb_r = cr, rgb_g = cg, rgb_b = cb;
-      if (colors_orig != nullptr && a.c_blend > 0.0f) {
-        const float* cm = colors_orig + (size_t)n * a.Ht * a.Wt * 3;
-        const float ux = x / a.scale, uy = y / a.scale;
-        const float upx = (float)px / a.scale, upy = (float)py / a.scale;
-        const float ur = r / a.scale;
-        const float3 co = psd_color_map(cm, a.Ht, a.Wt, upx - ux, upy - uy, ur, theta);
-        rgb_r = (1.0f - a.c_blend) * rgb_r + a.c_blend * co.x;
-        rgb_g = (1.0f - a.c_blend) * rgb_g + a.c_blend * co.y;
-        rgb_b = (1.0f - a.c_blend) * rgb_b + a.c_blend * co.z;
+    const int lpx = bx + lx;
+    if (lpx >= bw) continue;
+    const int px = bb.x + lpx;
+    const int rows = min(kPsdBlock, bh - by);   // rows of this block inside the crop
+    for (int ly = ly0; ly < rows; ly += 2) {
+      const int lpy = by + ly;
+      const int py = bb.y + lpy;
+      // The column is hidden from the optimiser in every row, so no part of
+      // the pixel's expression is hoisted out of the loop: a hoisted cos*u
+      // lets the compiler fuse the other product instead, which changes the
+      // fast-math rounding and, rarely, a byte against the reference kernel.
+      int pxr = px;
+      asm volatile("" : "+r"(pxr));
+      const float tv = psd_template_value(tmpl, t_idx, a.P, a.Ht, a.Wt, pxr, py, x, y, r, cos_t, sin_t);
+      const float alpha_val = tv * vs * a.alpha_max;
+      uchar4 px4 = make_uchar4(0, 0, 0, 0);
+      if (!(alpha_val < 0.001f)) {
+        float rgb_r = cr, rgb_g = cg, rgb_b = cb;
+        if (colors_orig != nullptr && a.c_blend > 0.0f) {
+          const float* cm = colors_orig + (size_t)n * a.Ht * a.Wt * 3;
+          const float ux = x / a.scale, uy = y / a.scale;
+          const float upx = (float)pxr / a.scale, upy = (float)py / a.scale;
+          const float ur = r / a.scale;
+          const float3 co = psd_color_map(cm, a.Ht, a.Wt, upx - ux, upy - uy, ur, theta);
+          rgb_r = (1.0f - a.c_blend) * rgb_r + a.c_blend * co.x;
+          rgb_g = (1.0f - a.c_blend) * rgb_g + a.c_blend * co.y;
+          rgb_b = (1.0f - a.c_blend) * rgb_b + a.c_blend * co.z;
+        }
+        const float mask = tv > 0.0f ? 1.0f : 0.0f;
+        px4 = make_uchar4(to_u8(mask * rgb_r), to_u8(mask * rgb_g), to_u8(mask * rgb_b), to_u8(alpha_val));
       }
-      const float mask = tv > 0.0f ? 1.0f : 0.0f;
-      px4 = make_uchar4(to_u8(mask * rgb_r), to_u8(mask * rgb_g), to_u8(mask * rgb_b), to_u8(alpha_val));
+      *reinterpret_cast<uchar4*>(out + off + ((long long)lpy * bw + lpx) * 4) = px4;
     }
-    *reinterpret_cast<uchar4*>(out + off + ((long long)lpy * bw + lpx) * 4) = px4;
   }
 }
 
@@ -476,16 +491,14 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
           const int n = min(32, w - x0);
           for (int x = 0; x < n; ++x) {
             const uint32_t p = sm[lane * kRlePitch + x];
-            // Count pass only: when all four bytes repeat, every run grows.  The
-            // write pass measured slower with this shortcut (24.7 -> 28.3 ms at
-            // 2048x2048, N=20000 on a B200) and the count pass faster (12.5 ->
-            // 8.2 ms); both give the same bytes.
-            if (!WRITE && (unsigned long long)p == last) {
+            // When all four bytes repeat, every run grows (2048x2048, N=20000 on
+            // a B200: count pass 12.5 -> 8.2 ms, write pass 14.7 -> 12.1 ms).
+            if ((unsigned long long)p == last) {
 #pragma unroll
               for (int s = 0; s < 4; ++s) ++e.run[s];
               continue;
             }
-            if (!WRITE) last = p;
+            last = p;
             any_alpha |= p & 0xFF000000u;
 #pragma unroll
             for (int s = 0; s < 4; ++s) e.push(s, (p >> (8 * ((a.order >> (8 * s)) & 3))) & 0xFF);
