@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 // match the data can write wrong bytes but never out of bounds.
 // ---------------------------------------------------------------------------
 
-constexpr int kRleWarps = 8;      // warps per CTA
+constexpr int kRleWarps = 4;      // warps per CTA (two staging buffers of 32 x 33 words each)
 constexpr int kRlePitch = 33;     // words per staged row (32 pixels + 1 pad)
 constexpr int kRleMaxWidth = 30000;
 
@@ -413,11 +413,24 @@ struct RleWrite {
   }
 };
 
+// One 4-byte asynchronous copy from global to shared memory (cp.async); with
+// valid false nothing is read and the word is zero-filled.
+__device__ __forceinline__ void cp_async_word(uint32_t* dst, const void* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory"); }
+
 template <bool WRITE>
 __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
-  __shared__ uint32_t stage[kRleWarps][32 * kRlePitch];
+  // Per warp, two staging buffers of 32 rows x 32 pixels: the copies of the
+  // next 32 columns of the group's rows are in flight while the lanes encode
+  // the current ones.
+  __shared__ uint32_t stage[kRleWarps][2][32 * kRlePitch];
   const int lane = threadIdx.x & 31;
-  uint32_t* sm = stage[threadIdx.x >> 5];
+  uint32_t(*sm)[32 * kRlePitch] = stage[threadIdx.x >> 5];
   const long long nwarps = (long long)gridDim.x * kRleWarps;
   for (long long g = (long long)blockIdx.x * kRleWarps + (threadIdx.x >> 5); g < a.G; g += nwarps) {
     int lo = 0, hi = a.N;   // largest i with group_base[i] <= g
@@ -477,20 +490,31 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
     uint32_t any_alpha = 0;
     unsigned long long last = 1ull << 32;   // the previous pixel; no pixel equals the initial value
     if (!skip) {   // warp-uniform: skip depends on the layer only
-      for (int x0 = 0; x0 < w; x0 += 32) {
-        __syncwarp();
-#pragma unroll 4
+      // columns x0 .. x0 + 31 of the group's 32 rows into buffer buf, one
+      // coalesced 128-byte row segment per copy instruction of the warp
+      auto stage_chunk = [&](int x0, uint32_t* buf) {
+#pragma unroll 8
         for (int r = 0; r < 32; ++r) {
-          uint32_t v = 0;
-          if (y0 + r < h && x0 + lane < w)
-            v = *reinterpret_cast<const uint32_t*>(base + ((y0 + r) * (long long)w + x0 + lane) * 4);
-          sm[r * kRlePitch + lane] = v;
+          const bool v = y0 + r < h && x0 + lane < w;
+          cp_async_word(buf + r * kRlePitch + lane, v ? base + ((y0 + r) * (long long)w + x0 + lane) * 4 : base, v);
         }
-        __syncwarp();
+        cp_async_commit();
+      };
+      __syncwarp();   // every lane is done with both buffers (previous group)
+      stage_chunk(0, sm[0]);
+      int cur = 0;
+      for (int x0 = 0; x0 < w; x0 += 32, cur ^= 1) {
+        if (x0 + 32 < w) {
+          stage_chunk(x0 + 32, sm[cur ^ 1]);   // read by every lane in the previous iteration
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
+        }
+        __syncwarp();   // the lanes' copies of this chunk are visible to the whole warp
         if (active) {
           const int n = min(32, w - x0);
           for (int x = 0; x < n; ++x) {
-            const uint32_t p = sm[lane * kRlePitch + x];
+            const uint32_t p = sm[cur][lane * kRlePitch + x];
             // When all four bytes repeat, every run grows (2048x2048, N=20000 on
             // a B200: count pass 12.5 -> 8.2 ms, write pass 14.7 -> 12.1 ms).
             if ((unsigned long long)p == last) {
@@ -504,6 +528,7 @@ __global__ void __launch_bounds__(kRleWarps * 32) psd_rle_kernel(RleArgs a) {
             for (int s = 0; s < 4; ++s) e.push(s, (p >> (8 * ((a.order >> (8 * s)) & 3))) & 0xFF);
           }
         }
+        __syncwarp();   // every lane is done with this buffer before the next iteration refills it
       }
       if (active) {
 #pragma unroll
