@@ -81,65 +81,65 @@ __global__ void psd_layout_kernel(const int* __restrict__ sizes, int N, long lon
   }
 }
 
-// Template value at canvas pixel (px,py): psd_export_common.h:55-103 (u from
-// (px - x) / r, hard zero when u_t < 0 or u_t >= W-1).
+// Template value at canvas pixel (px,py): psd_export_common.h:55-103, with
+// each floating-point operation in the reference's order (the layers must be
+// byte-identical under --use_fast_math).  The texel coordinate (sx, sy) comes
+// from (px - x) / r rotated by theta; outside [0, W-1) x [0, H-1) the value is
+// a hard zero.  After that test the cell (ix, iy) = floor(sx, sy) lies in
+// [0, W-2] x [0, H-2] (a NaN coordinate converts to cell 0), so it needs no
+// clamp, and the weights take the floors as floats, which equal the cell
+// indices exactly.
 __device__ __forceinline__ float psd_template_value(const float* __restrict__ tmpl, int t_idx, int P, int Ht, int Wt,
                                                     int px, int py, float x, float y, float r, float cos_t,
                                                     float sin_t) {
-  const float u_norm = ((float)px - x) / (r);
-  const float v_norm = ((float)py - y) / (r);
-  const float u_rot = cos_t * u_norm + sin_t * v_norm;
-  const float v_rot = -sin_t * u_norm + cos_t * v_norm;
-  const float u_t = (u_rot + 1.0f) * 0.5f * (Wt - 1);
-  const float v_t = (v_rot + 1.0f) * 0.5f * (Ht - 1);
-  if (u_t < 0.0f || u_t >= Wt - 1 || v_t < 0.0f || v_t >= Ht - 1) return 0.0f;
+  const float qx = ((float)px - x) / (r);
+  const float qy = ((float)py - y) / (r);
+  const float ex = cos_t * qx + sin_t * qy;
+  const float ey = -sin_t * qx + cos_t * qy;
+  const float sx = (ex + 1.0f) * 0.5f * (Wt - 1);
+  const float sy = (ey + 1.0f) * 0.5f * (Ht - 1);
+  if (sx < 0.0f || sx >= Wt - 1 || sy < 0.0f || sy >= Ht - 1) return 0.0f;
   if (t_idx < 0 || t_idx >= P) return 0.0f;   // the reference reads out of bounds here
-  int u0 = (int)floorf(u_t);
-  int v0 = (int)floorf(v_t);
-  u0 = max(0, min(u0, Wt - 1));
-  v0 = max(0, min(v0, Ht - 1));
-  const float wu = u_t - u0;
-  const float wv = v_t - v0;
-  const float wu_inv = 1.0f - wu;
-  const float wv_inv = 1.0f - wv;
-  const float* t = tmpl + (size_t)t_idx * Ht * Wt;
-  const float v00 = t[v0 * Wt + u0];
-  const float v01 = t[v0 * Wt + u0 + 1];
-  const float v10 = t[(v0 + 1) * Wt + u0];
-  const float v11 = t[(v0 + 1) * Wt + u0 + 1];
-  return wu_inv * wv_inv * v00 + wu * wv_inv * v01 + wu_inv * wv * v10 + wu * wv * v11;
+  const float flx = floorf(sx), fly = floorf(sy);
+  const int ix = (int)flx, iy = (int)fly;
+  const float fx = sx - flx;
+  const float fy = sy - fly;
+  const float gx = 1.0f - fx;
+  const float gy = 1.0f - fy;
+  const float* row = tmpl + (size_t)t_idx * Ht * Wt + iy * Wt + ix;
+  const float s00 = row[0], s01 = row[1], s10 = row[Wt], s11 = row[Wt + 1];
+  return gx * gy * s00 + fx * gy * s01 + gx * fy * s10 + fx * fy * s11;
 }
 
-// Clamped bilinear of a per-primitive RGB map (psd_export_common.h:124-196),
-// used only with c_blend > 0.
+// Clamped bilinear of a per-primitive RGB map (psd_export_common.h:124-196,
+// operations in its order), used only with c_blend > 0: the coordinate is
+// clamped into the map and the neighbours past the last row / column repeat it.
 __device__ __forceinline__ float3 psd_color_map(const float* __restrict__ cm, int map_h, int map_w, float x, float y,
                                                 float radius, float rotation) {
-  float r_inv = radius > 1e-6f ? (1.0f / radius) : 1e6f;
-  float norm_x = x * r_inv;
-  float norm_y = y * r_inv;
-  float cos_theta = cosf(rotation);
-  float sin_theta = sinf(rotation);
-  float rot_x = cos_theta * norm_x + sin_theta * norm_y;
-  float rot_y = -sin_theta * norm_x + cos_theta * norm_y;
-  float coord_x = (rot_x + 1.0f) * 0.5f * (map_w - 1);
-  float coord_y = (rot_y + 1.0f) * 0.5f * (map_h - 1);
-  coord_x = fmaxf(0.0f, fminf(map_w - 1, coord_x));
-  coord_y = fmaxf(0.0f, fminf(map_h - 1, coord_y));
-  int x0 = (int)coord_x;
-  int y0 = (int)coord_y;
-  int x1 = min(x0 + 1, map_w - 1);
-  int y1 = min(y0 + 1, map_h - 1);
-  float fx = coord_x - x0;
-  float fy = coord_y - y0;
+  const float inv = radius > 1e-6f ? (1.0f / radius) : 1e6f;
+  const float qx = x * inv;
+  const float qy = y * inv;
+  const float ct = cosf(rotation);
+  const float st = sinf(rotation);
+  const float ex = ct * qx + st * qy;
+  const float ey = -st * qx + ct * qy;
+  float sx = (ex + 1.0f) * 0.5f * (map_w - 1);
+  float sy = (ey + 1.0f) * 0.5f * (map_h - 1);
+  sx = fmaxf(0.0f, fminf(map_w - 1, sx));
+  sy = fmaxf(0.0f, fminf(map_h - 1, sy));
+  const int ix = (int)sx, iy = (int)sy;
+  const int jx = min(ix + 1, map_w - 1), jy = min(iy + 1, map_h - 1);
+  const float fx = sx - ix;
+  const float fy = sy - iy;
   float3 out;
   float* o = &out.x;
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) {
-    const float c00 = cm[3 * (y0 * map_w + x0) + ch], c01 = cm[3 * (y1 * map_w + x0) + ch];
-    const float c10 = cm[3 * (y0 * map_w + x1) + ch], c11 = cm[3 * (y1 * map_w + x1) + ch];
-    const float c0 = c00 * (1.0f - fx) + c10 * fx;
-    const float c1 = c01 * (1.0f - fx) + c11 * fx;
-    o[ch] = c0 * (1.0f - fy) + c1 * fy;
+    const float a0 = cm[3 * (iy * map_w + ix) + ch], b0 = cm[3 * (jy * map_w + ix) + ch];
+    const float a1 = cm[3 * (iy * map_w + jx) + ch], b1 = cm[3 * (jy * map_w + jx) + ch];
+    const float top = a0 * (1.0f - fx) + a1 * fx;
+    const float bot = b0 * (1.0f - fx) + b1 * fx;
+    o[ch] = top * (1.0f - fy) + bot * fy;
   }
   return out;
 }
