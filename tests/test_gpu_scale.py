@@ -12,6 +12,8 @@
   (boundary band held to its spread), the same against the reference's own
   kernels (K = deepest pixel + 16), and the fused fit step (forward + L2 loss
   gradient + backward in one kernel) for FP32 / FP16 / BF16 quad storage.
+* The 2048x2048 / N=20000 fit step of the benchmark: the fused kernel's loss
+  and gradient sums equal the unfused kernels' on the same FP16 / BF16 atlas.
 """
 import ctypes
 
@@ -229,3 +231,31 @@ def test_c1_fused_step_vs_oracle_gpu(c1, c1_loss_grad, kind, min_psnr, grad_rel)
         spread = np.linalg.norm(g[1e-3][:, k] - g[-1e-3][:, k])
         print(f"  block {k}: rel err {e / nrm:.2e}, band {spread / nrm:.2e}")
         assert e <= grad_rel * nrm + spread
+
+
+@pytest.mark.parametrize("kind", ["f16q", "bf16q"])
+def test_c2_fused_step_equals_plain_kernels_gpu(kind):
+    """The headline kernel at its full size (2048x2048, N=20000, 16 templates
+    of 256^2 in FP16 / BF16 quads): the fused forward + L2 gradient + backward
+    gives the loss and the eight per-primitive gradient sums of the unfused
+    forward kernel, the torch L2 gradient and the backward kernel on the same
+    atlas and lists (the two differ only in the order of FP64 additions and
+    in where 2 (C - target) / n is rounded)."""
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.fitting import FitConfig, ImageFitter
+    from diffbmp_b200.rasterizer import Atlas
+    s = wl.make_scene("c2", seed=0)
+    atlas = Atlas(torch.from_numpy(s.templates).cuda(), kind)
+    jobs = [ImageFitter(s.means2D, s.radii, s.rotations, s.opacities, s.colors, s.sel, atlas, s.target,
+                        s.background, FitConfig(fused=fused)) for fused in (True, False)]
+    for j in jobs:
+        j.adam_cfg.lr[:] = [0.0] * 8          # parameters stay put: gradients only
+        j.step()
+        j.sync()
+        assert int(j.flags[1].item()) == 0    # the lists fitted their capacity
+    ga, gb = (j.gacc.cpu().numpy() for j in jobs)
+    for k in range(8):
+        rel = np.linalg.norm(ga[:, k] - gb[:, k]) / max(np.linalg.norm(gb[:, k]), 1e-30)
+        assert rel < 1e-5, (k, rel)
+    la, lb = jobs[0].loss(), jobs[1].loss()
+    assert abs(la - lb) <= 1e-6 * lb, (la, lb)
