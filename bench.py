@@ -768,7 +768,8 @@ def main():
                         "one step in flight"},
         "gpu_launches": 6 * args.steps,
         "gpu_launches_note": "ours per step: prepare, counts, bin_rows, fused, adam, step_increment "
-                             "(+ one memset and the two kernels of one CUB exclusive scan over the tile counts)",
+                             "(+ three memsets -- the binning difference arrays, the loss and the gradient "
+                             "sums -- and the two kernels of one CUB exclusive scan over the tile counts)",
         "clocks": clocks,
     }
     if args.serving_jobs > 0 and world == 1:   # the serving stream is a single-GPU measurement
