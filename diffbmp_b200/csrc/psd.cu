@@ -285,7 +285,9 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 // 32 at a time, one warp per group of 32 rows of a layer and one lane per
 // row; each lane runs four encoders at once, one per RGBA byte, on uchar4
 // pixels that the warp stages through shared memory 32 rows x 32 pixels at a
-// time (coalesced loads, conflict-free reads with a 33-word row pitch).
+// time (cp.async copies of coalesced row segments into two buffers, the next
+// chunk in flight while the current one is encoded; conflict-free reads with
+// a 33-word row pitch).
 //
 // Encoding rule (a valid PackBits stream; a packet never crosses a row):
 //   - a maximal run of L >= 3 equal bytes becomes replicate packets
@@ -294,7 +296,8 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 //   - maximal runs of one or two bytes are gathered into literal segments,
 //     written as packets [k-1, k bytes] of 128 bytes and a last shorter one.
 // The count pass writes each row's encoded size (at most w + ceil(w/128)
-// bytes, so 16 bits suffice for w <= 30000, the PSD width limit) and each
+// bytes, so 16 bits suffice for w <= 30000, the PSD width limit that the C
+// ABI enforces on width_limit) and each
 // group's per-channel totals; the host plans where every channel block goes;
 // the write pass re-encodes and stores.  Each store is checked against the
 // planned extent of its row and the output size, so a plan that does not
@@ -303,7 +306,6 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 
 constexpr int kRleWarps = 4;      // warps per CTA (two staging buffers of 32 x 33 words each)
 constexpr int kRlePitch = 33;     // words per staged row (32 pixels + 1 pad)
-constexpr int kRleMaxWidth = 30000;
 
 struct RleArgs {
   const uint8_t* layers;        // packed RGBA crops, row-major per layer
