@@ -2,7 +2,8 @@
 
 * The device PackBits channel blocks (dbmp_psd_rle_count / _write through
   ``encode_channel_blocks``) are byte-identical to the oracle's encoder on
-  ragged images, both channel orders and partial selections.
+  ragged images, both channel orders and partial selections, and to its
+  compiled restatement on the 1024x1024 / N=5000 export case.
 * ``PSDExporter`` writes a file that the oracle reader decodes to exactly the
   layers ``export_psd_layers_uint8`` returns (whose bytes the reference-kernel
   tests pin), with the reference's order (background at the bottom, primitive
@@ -79,6 +80,42 @@ def test_rle_blocks_match_oracle(order, pick):
     got = blob.cpu().numpy().tobytes()
     assert got == exp
     assert int(blocks.sum()) == len(exp)
+
+
+def test_rle_blocks_full_size_match_compiled_encoder():
+    """The 1024x1024 / N=5000 export case (8 templates of 128^2, radii s W / 2
+    with s log-uniform in [0.05, 0.3]; 1.0 GB of crops): every kept layer's
+    four channel blocks, as the device's count and write passes produce them,
+    are byte-identical to the compiled restatement of the encoder run on the
+    same crops."""
+    import diffbmp_b200.psd as P
+    from diffbmp_b200 import workloads as wl
+    W, N, n_tmpl, S = 1024, 5000, 8, 128
+    rng = np.random.default_rng(0)
+    tm = torch.from_numpy(np.stack([wl.random_shape(rng, S) for _ in range(n_tmpl)])).cuda()
+    t = lambda a: torch.from_numpy(np.asarray(a, np.float32)).cuda()
+    m = t(np.stack([rng.uniform(0, W, N), rng.uniform(0, W, N)], 1))
+    r = t(np.exp(rng.uniform(np.log(0.05), np.log(0.3), N)) * W / 2)
+    th = t(rng.uniform(0, 2 * np.pi, N))
+    vs = torch.sigmoid(t(rng.normal(0, 1, N)))
+    cs = torch.sigmoid(t(rng.normal(0, 2, (N, 3))))
+    sel = torch.from_numpy(((N - 1 - np.arange(N)) % n_tmpl).astype(np.int32)).cuda()
+    buf, bbox, sizes, offs = P.export_layers(tm, m, r, th, vs, cs, sel, W, W)
+    hs = sizes.cpu().numpy()
+    blob, blocks, chosen = P.encode_channel_blocks(buf, sizes, offs, hs, P.ORDER_LAYER,
+                                                   lambda flags: np.nonzero(flags)[0])
+    crops, o, got = buf.cpu().numpy(), offs.cpu().numpy(), blob.cpu().numpy()
+    assert len(chosen) > 0.9 * N
+    pos = 0
+    for i in chosen:
+        w, h = int(hs[i][0]), int(hs[i][1])
+        im = crops[o[i]:o[i] + w * h * 4].reshape(h, w, 4)
+        for slot in range(4):
+            data, rows = O.packbits_rows_c(im[:, :, (P.ORDER_LAYER >> (8 * slot)) & 3])
+            exp = b"\x00\x01" + rows.astype(">u2").tobytes() + data
+            assert got[pos:pos + len(exp)].tobytes() == exp, (int(i), slot)
+            pos += len(exp)
+    assert pos == got.size
 
 
 def test_rle_repeated_calls_identical():
