@@ -49,11 +49,33 @@ def _psd_case(seed, N, H, W, scale, c_blend):
     return tm, np.stack([x, y], 1), r, th, v, c, sel, co
 
 
+def _export_case(N, W):
+    """The benchmark's PSD export case on a W x W canvas: 8 templates of
+    128^2, centres uniform over the canvas, radii s W / 2 with s log-uniform
+    in [0.05, 0.3], rotations uniform in [0, 2 pi)."""
+    rng = np.random.default_rng(0)
+    from diffbmp_b200 import workloads as wl
+    P = 8
+    tm = np.stack([wl.random_shape(rng, 128) for _ in range(P)])
+    m = np.stack([rng.uniform(0, W, N), rng.uniform(0, W, N)], 1)
+    r = np.exp(rng.uniform(np.log(0.05), np.log(0.3), N)) * W / 2
+    th = rng.uniform(0, 2 * np.pi, N)
+    v = 1 / (1 + np.exp(-rng.normal(0, 1, N)))
+    c = 1 / (1 + np.exp(-rng.normal(0, 2, (N, 3))))
+    sel = ((N - 1 - np.arange(N)) % P).astype(np.int32)
+    return tm, m, r, th, v, c, sel, None
+
+
 @pytest.mark.parametrize("seed,N,H,W,scale,c_blend", [(0, 300, 256, 256, 1.0, 0.0), (1, 200, 200, 136, 2.0, 0.0),
-                                                      (2, 150, 160, 192, 1.0, 0.35), (3, 64, 96, 96, 0.5, 1.0)])
+                                                      (2, 150, 160, 192, 1.0, 0.35), (3, 64, 96, 96, 0.5, 1.0),
+                                                      (None, 5000, 1024, 1024, 1.0, 0.0)])
 def test_psd_bit_exact_vs_reference_kernel(seed, N, H, W, scale, c_blend):
+    """Crop boxes, offsets and layer bytes against the reference's own
+    kernels; the last case is the benchmark's 1024x1024 / N=5000 export
+    (1.0 GB of crops)."""
     from diffbmp_b200.psd import export_layers
-    tm, m, r, th, v, c, sel, co = _psd_case(seed, N, H, W, scale, c_blend)
+    tm, m, r, th, v, c, sel, co = _psd_case(seed, N, H, W, scale, c_blend) if seed is not None else \
+        _export_case(N, W)
     P, Ht, Wt = tm.shape
     t_tm, t_m, t_r, t_th, t_v, t_c = dev(tm), dev(m), dev(r), dev(th), dev(v), dev(c)
     t_sel = dev(sel, np.int32)
@@ -68,7 +90,9 @@ def test_psd_bit_exact_vs_reference_kernel(seed, N, H, W, scale, c_blend):
     torch.cuda.synchronize()
     assert torch.equal(rb, bbox) and torch.equal(rs, sizes)
     hs = rs.cpu().numpy()
-    ro = np.concatenate([[0], np.cumsum(hs[:, 0].astype(np.int64) * hs[:, 1] * 4)[:-1]]).astype(np.int32)
+    ro64 = np.concatenate([[0], np.cumsum(hs[:, 0].astype(np.int64) * hs[:, 1] * 4)[:-1]])
+    assert ro64[-1] < 2 ** 31                      # the reference's offsets are 32-bit
+    ro = ro64.astype(np.int32)
     assert np.array_equal(ro, offs.cpu().numpy())
     total = int((hs[:, 0].astype(np.int64) * hs[:, 1] * 4).sum())
     rbuf = torch.zeros(total, dtype=torch.uint8, device="cuda")
