@@ -2,7 +2,7 @@
 from the reference sources into oracle/_ref/ by `make -C oracle ref`) beside
 this repository's kernels on the same scenes and the same GPU.
 
-    python oracle/time_reference_gpu.py [--configs c0,c1] [--reps 20]
+    python oracle/time_reference_gpu.py [--configs c0,c1] [--reps 20] [--psd 1024:5000]
 
 Per config it prints one JSON line with:
 * ref_fwd_bwd_ms: one reference forward + backward as the reference runs it
@@ -190,16 +190,79 @@ def time_config(cfg, reps):
     return out
 
 
+def time_psd(W, N, reps):
+    """The PSD crop kernels on the export case of a W x W canvas with N
+    primitives (8 templates of 128^2, centres uniform, radii s W / 2 with s
+    log-uniform in [0.05, 0.3]): the reference's generate_cropped_layers
+    launch (psd_export_kernels.cu:219-270, one thread per primitive for every
+    16x16 tile of the canvas) and this repository's dbmp_psd_layers on the
+    same boxes and offsets, each timed with CUDA events over `reps` launches."""
+    from diffbmp_b200 import workloads as wl
+    from diffbmp_b200.psd import export_layers
+    from diffbmp_b200._lib import call
+    from diffbmp_b200.rasterizer import _ptr, _stream
+    rng = np.random.default_rng(0)
+    P, S = 8, 128
+    tm = dev(np.stack([wl.random_shape(rng, S) for _ in range(P)]))
+    m = dev(np.stack([rng.uniform(0, W, N), rng.uniform(0, W, N)], 1))
+    r = dev(np.exp(rng.uniform(np.log(0.05), np.log(0.3), N)) * W / 2)
+    th = dev(rng.uniform(0, 2 * np.pi, N))
+    v = dev(1 / (1 + np.exp(-rng.normal(0, 1, N))))
+    c = dev(1 / (1 + np.exp(-rng.normal(0, 2, (N, 3)))))
+    sel = dev((N - 1 - np.arange(N)) % P, np.int32)
+    buf, bbox, sizes, offs = export_layers(tm, m, r, th, v, c, sel, W, W, 1.0, 0.9, 0.0, None)
+    hs = sizes.cpu().numpy()
+    total = int((hs[:, 0].astype(np.int64) * hs[:, 1] * 4).sum())
+    out = {"psd_case": f"{W}x{W}, N={N}", "crop_bytes": total}
+    if total >= 2 ** 31:
+        out["ref_skipped"] = "the reference's layer offsets are 32-bit and the crops exceed 2^31 bytes"
+        return out
+    ro = dev(np.concatenate([[0], np.cumsum(hs[:, 0].astype(np.int64) * hs[:, 1] * 4)[:-1]]), np.int32)
+    rbuf = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    L = RG.psd()
+    blk = torch.zeros(N + 1, dtype=torch.int64, device="cuda")
+    lo = torch.zeros(N, dtype=torch.int64, device="cuda")
+    tb = torch.zeros(1, dtype=torch.int64, device="cuda")
+    call("dbmp_psd_layout", _ptr(sizes), N, _ptr(lo), _ptr(blk), _ptr(tb), _stream())
+
+    def ref():
+        L.launch_generate_cropped_layers(P_(m), P_(r), P_(th), P_(c), P_(v), P_(tm), P_(sel), P_(bbox), P_(ro),
+                                         P_(rbuf), N, W, W, S, S, ctypes.c_float(1.0), ctypes.c_float(0.9),
+                                         ctypes.c_float(0.0), None, W, W)
+
+    def ours():
+        call("dbmp_psd_layers", _ptr(m), _ptr(r), _ptr(th), _ptr(c), _ptr(v), _ptr(tm), P, S, S, _ptr(sel),
+             _ptr(bbox), _ptr(lo), _ptr(blk), N, ctypes.c_float(1.0), ctypes.c_float(0.9), ctypes.c_float(0.0), None,
+             _ptr(buf), _stream())
+
+    for name, fn in (("ref_psd_layers_ms", ref), ("ours_psd_layers_ms", ours)):
+        fn(); torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record(); e1.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    out["bytes_equal"] = bool(torch.equal(rbuf, buf))
+    out["speedup"] = out["ref_psd_layers_ms"] / out["ours_psd_layers_ms"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--configs", default="c0,c1")
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--psd", default="", help="PSD crop cases W:N,... (e.g. 1024:5000,2048:20000)")
     a = ap.parse_args()
     if not RG.available():
         print(json.dumps({"unavailable": "reference kernels not built (make -C oracle ref)"}))
         return
-    for cfg in a.configs.split(","):
+    for cfg in [c for c in a.configs.split(",") if c]:
         print(json.dumps(time_config(cfg, a.reps)), flush=True)
+        torch.cuda.empty_cache()
+    for case in [c for c in a.psd.split(",") if c]:
+        W, N = (int(x) for x in case.split(":"))
+        print(json.dumps(time_psd(W, N, a.reps)), flush=True)
         torch.cuda.empty_cache()
 
 
