@@ -13,7 +13,9 @@
   kernels (K = deepest pixel + 16), and the fused fit step (forward + L2 loss
   gradient + backward in one kernel) for FP32 / FP16 / BF16 quad storage.
 * The 2048x2048 / N=20000 fit step of the benchmark: the fused kernel's loss
-  and gradient sums equal the unfused kernels' on the same FP16 / BF16 atlas.
+  and gradient sums equal the unfused kernels' on the same FP16 / BF16 atlas,
+  and the FP16 / BF16-storage image is at >= 60 dB against the FP64 oracle
+  on a band of 8 tile rows.
 """
 import ctypes
 
@@ -259,3 +261,47 @@ def test_c2_fused_step_equals_plain_kernels_gpu(kind):
         assert rel < 1e-5, (k, rel)
     la, lb = jobs[0].loss(), jobs[1].loss()
     assert abs(la - lb) <= 1e-6 * lb, (la, lb)
+
+
+def test_c2_precision_band_vs_oracle_gpu():
+    """The precision target at the benchmark's size (2048x2048, N=20000, 16
+    templates of 256^2): the image rendered with FP16 and with BF16 quad
+    storage (opacities and colours in FP16 in the records), composited over
+    the scene's background, is at >= 60 dB PSNR against the FP64 oracle on 8
+    tile rows at the middle of the canvas (pixel rows 896-1151, full width);
+    the FP32 reference-layout render is within 1e-4 max-abs there.  The band
+    is rendered by the oracle from the full canvas's tile lists with the
+    centres shifted by the band's first row in float64, which leaves every
+    pixel's arithmetic unchanged."""
+    from diffbmp_b200 import workloads as wl
+    s = wl.make_scene("c2", seed=0)
+    ts, y0, y1 = 32, 896, 1152
+    imgs = {}
+    for kind in ("f32", "f16q", "bf16q"):
+        atlas = R.Atlas(_t(s.templates), kind)
+        rz = R.Rasterizer(s.H, s.W, ts)
+        color, alpha, _ = rz.forward(_t(s.means2D), _t(s.radii), _t(s.rotations), _t(s.opacities), _t(s.colors),
+                                     _t(s.sel, np.int32), atlas)
+        imgs[kind] = (color[y0:y1].cpu().numpy().astype(np.float64), alpha[y0:y1].cpu().numpy().astype(np.float64))
+        del color, alpha, atlas, rz
+    tb = O.template_bboxes(s.templates)
+    P, Ht, Wt = s.templates.shape
+    offs, idx = O.bin_tiles(s.H, s.W, ts, s.means2D, s.radii, s.rotations, s.sel, tb, Ht, Wt)
+    tx = (s.W + ts - 1) // ts
+    t0, t1 = (y0 // ts) * tx, (y1 // ts) * tx
+    so = (offs[t0:t1 + 1] - offs[t0]).astype(np.int32)
+    si = idx[offs[t0]:offs[t1]]
+    m = s.means2D.astype(np.float64).copy()
+    m[:, 1] -= y0
+    ref = O.forward(O.Scene(y1 - y0, s.W, ts, m, s.radii, s.rotations, s.opacities, s.colors, s.templates, s.sel,
+                            s.alpha_max), so, si)
+    bg = s.background[y0:y1].astype(np.float64)
+    ref_img = ref["color"] + (1.0 - ref["alpha"])[..., None] * bg
+    for kind, (color, alpha) in imgs.items():
+        err = np.abs(color + (1.0 - alpha)[..., None] * bg - ref_img)
+        psnr = 10 * np.log10(1.0 / max(float(np.mean(err ** 2)), 1e-30))
+        print(f"{kind}: PSNR {psnr:.1f} dB, max-abs {err.max():.2e}")
+        if kind == "f32":
+            assert err.max() <= 1e-4 and np.abs(alpha - ref["alpha"]).max() <= 1e-4
+        else:
+            assert psnr >= 60.0, (kind, psnr)
