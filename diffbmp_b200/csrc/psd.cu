@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 // pixels that the warp stages through shared memory 32 rows x 32 pixels at a
 // time (cp.async copies of coalesced row segments into two buffers, the next
 // chunk in flight while the current one is encoded; conflict-free reads with
-// a 33-word row pitch).
+// a 36-word row pitch, four pixels per 16-byte read).
 //
 // Encoding rule (a valid PackBits stream; a packet never crosses a row):
 //   - a maximal run of L >= 3 equal bytes becomes replicate packets
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
 // match the data can write wrong bytes but never out of bounds.
 // ---------------------------------------------------------------------------
 
-constexpr int kRleWarps = 4;      // warps per CTA (two staging buffers of 32 x 33 words each)
+constexpr int kRleWarps = 4;      // warps per CTA (two staging buffers of 32 x 36 words each)
 // Words per staged row: 32 pixels + 4 pad.  Row starts 144 bytes apart keep
 // the staging copies (32 consecutive words of a row) and each lane's 16-byte
 // reads of its own row (8 lanes per phase on distinct 16-byte bank groups)
