@@ -239,10 +239,38 @@ __global__ void __launch_bounds__(256) psd_layers_kernel(PsdArgs a, const float*
       if (bx >= bb.z - bb.x) { bx = 0; by += kPsdBlock; }
     }
     const int bw = bb.z - bb.x, bh = bb.w - bb.y;
+    // Warp-uniform: true when the whole block maps outside the template
+    // square [-1, 1) x [-1, 1) of the normalised frame (rotated (p - c) / r)
+    // by a margin of 1e-3, far above the rounding of the per-pixel
+    // coordinates; each of its pixels then takes the hard zero, and its bytes
+    // are stored as zeros without the per-pixel arithmetic.  The map is affine,
+    // so the block's four corner pixels bound it.  Only for finite inputs with
+    // r > 1e-3: a non-finite coordinate or opacity can give nonzero bytes.
+    bool outside = false;
+    if (r > 1e-3f && isfinite(r) && isfinite(x) && isfinite(y) && isfinite(cos_t) && isfinite(sin_t) &&
+        isfinite(vs) && isfinite(a.alpha_max)) {
+      const float inv = 1.0f / r;
+      const float qx0 = ((float)(bb.x + bx) - x) * inv, qx1 = ((float)(bb.x + bx + kPsdBlock - 1) - x) * inv;
+      const float qy0 = ((float)(bb.y + by) - y) * inv, qy1 = ((float)(bb.y + by + kPsdBlock - 1) - y) * inv;
+      const float ex00 = cos_t * qx0 + sin_t * qy0, ex10 = cos_t * qx1 + sin_t * qy0;
+      const float ex01 = cos_t * qx0 + sin_t * qy1, ex11 = cos_t * qx1 + sin_t * qy1;
+      const float ey00 = cos_t * qy0 - sin_t * qx0, ey10 = cos_t * qy0 - sin_t * qx1;
+      const float ey01 = cos_t * qy1 - sin_t * qx0, ey11 = cos_t * qy1 - sin_t * qx1;
+      const float m = 1e-3f;
+      outside = fmaxf(fmaxf(ex00, ex10), fmaxf(ex01, ex11)) < -1.0f - m ||
+                fminf(fminf(ex00, ex10), fminf(ex01, ex11)) > 1.0f + m ||
+                fmaxf(fmaxf(ey00, ey10), fmaxf(ey01, ey11)) < -1.0f - m ||
+                fminf(fminf(ey00, ey10), fminf(ey01, ey11)) > 1.0f + m;
+    }
     const int lpx = bx + lx;
     if (lpx >= bw) continue;
     const int px = bb.x + lpx;
     const int rows = min(kPsdBlock, bh - by);   // rows of this block inside the crop
+    if (outside) {
+      for (int ly = ly0; ly < rows; ly += 2)
+        *reinterpret_cast<uchar4*>(out + off + ((long long)(by + ly) * bw + lpx) * 4) = make_uchar4(0, 0, 0, 0);
+      continue;
+    }
     for (int ly = ly0; ly < rows; ly += 2) {
       const int lpy = by + ly;
       const int py = bb.y + lpy;
