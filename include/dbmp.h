@@ -274,10 +274,10 @@ int dbmp_count(const dbmp_canvas* cv, const void* prim_info, const void* atlas,
                const int32_t* tile_offsets, const int32_t* tile_indices,
                unsigned long long* counts, void* stream);
 
-/* Fused forward + L2 loss + backward of one image-fitting iteration, one
- * CTA per tile: the forward walk composites, the CTA forms the reference
- * loss gradient of rendered = C + (1-A)*background against `target`
- * (mse_loss, pydiffbmp/util/loss_functions.py:20-40 on
+/* Fused forward + L2 loss + backward of one image-fitting iteration in one
+ * launch: each warp composites its pixels of a tile, forms the reference
+ * loss gradient of rendered = C + (1-A)*background against `target` for
+ * them (mse_loss, pydiffbmp/util/loss_functions.py:20-40 on
  * simple_tile_renderer.py:704-707) and walks the same list back.  Zeroes and
  * fills grad_accum ((N,8) f64 raw per-primitive sums, consumed by
  * dbmp_adam_step) and *loss_out (device f64, mean squared error).
