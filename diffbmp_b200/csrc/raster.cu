@@ -508,7 +508,7 @@ struct TileWalker {
   // Phase 2 of a forward entry: blend the loaded texels and composite.
   // Returns true when every pixel of the warp has stopped.
   __device__ __forceinline__ bool pair_composite(const Geom& g, const Rec* w, int e, int pos, const PairPre<KIND>& p,
-                                                 PairFwd& f) const {
+                                                 PairFwd& f, bool vote = true) const {
     const float4 c0 = w[e][2];
     const float4 c1 = w[e][3];
     PairSample s;
@@ -530,7 +530,7 @@ struct TileWalker {
     f.t.y = __saturatef(fmaf(-f.t.y, a.y, f.t.y));
     f.live[0] = f.live[0] && !(f.t.x < g.t_stop);
     f.live[1] = f.live[1] && !(f.t.y < g.t_stop);
-    return __all_sync(kFull, !f.live[0] && !f.live[1]);
+    return vote && __all_sync(kFull, !f.live[0] && !f.live[1]);
   }
 
   // Forward walk of the pixel-pair form: the walk of forward() with both
@@ -561,7 +561,9 @@ struct TileWalker {
         PairPre<KIND> p1, p2;
         pair_issue(g, atlas, w, e1, cm, f.live, p1);
         pair_issue(g, atlas, w, e2, cm, f.live, p2);
-        if (pair_composite(g, w, e1, base - start + e1, p1, f)) { warp_done = true; break; }
+        // one termination vote per pair: a pixel that stops at e1 has live
+        // false, so e2 composites nothing for it
+        if (pair_composite(g, w, e1, base - start + e1, p1, f, !two)) { warp_done = true; break; }
         if (two && pair_composite(g, w, e2, base - start + e2, p2, f)) { warp_done = true; break; }
       }
     }
